@@ -1,0 +1,375 @@
+"""SpMV benchmark: GB/s and fraction of the HBM roofline on one B200.
+
+Workload (default): FP32 CSR SpMV, 1D row partitions with nnz balance (the
+GPU planner's auto items), on the 1,048,576 x 1,048,576 Zipf power-law matrix
+(row lengths Zipf(2.0) capped at 50,000, mean 16, 16,777,216 nonzeros,
+uniform distinct columns, values and x U[-1, 1], seed 1), synthetic.
+
+One step = one SpMV over the whole matrix (inputs resident in HBM).  The L2
+(126 MB) is flushed before every timed step by writing a 256 MB buffer; each
+step is timed with CUDA events on the launching stream.  `value` is
+compulsory bytes / device time summed over all ranks' steps (replicas, weak
+scaling).  `e2e` is the same metric through sparsep_execute_host: pinned host
+x in, pinned host y out, copies inside the timed region.
+
+--impl reference times the reference's own host SpMV (spmv_host of
+spmv/1D/CSR-row/host/app.c, compiled from the reference sources into
+oracle/_ref) on the box's host cores: row slices of the matrix run the
+unchanged reference loop on all threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "zipf-1M-csr-f32-1d"
+METRIC = "SpMV GB/s (compulsory bytes / kernel time), FP32 CSR, 1M-row Zipf power-law matrix"
+FALLBACK_HBM = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", FALLBACK_HBM)), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+def make_matrix():
+    import sparsep_b200 as sp
+
+    t0 = time.time()
+    n, m, rows, cols, vals, x = sp.synth.zipf_rows(seed=1, dtype=np.float32)
+    rowptr, colind, values = sp.synth.to_csr(n, rows, cols, vals)
+    log(f"[bench] generated zipf matrix {n}x{m} nnz={rows.size} in {time.time() - t0:.1f}s "
+        f"(max row {int(np.diff(rowptr.astype(np.int64)).max())})")
+    return n, m, rowptr, colind, values, x
+
+
+def compulsory_bytes(n, m, nnz, s=4):
+    return nnz * (4 + s) + (n + 1) * 4 + m * s + n * s
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = []
+        for ln in (getattr(self, "out", "") or "").splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) >= 9:
+                try:
+                    rows.append((float(f[1]), float(f[2]), f[5:9]))
+                except ValueError:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+
+    import sparsep_b200 as sp
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    n, m, rowptr, colind, values, x = make_matrix()
+    nnz = int(rowptr[-1])
+    A = sp.csr("f32", n, m, rowptr, colind, values)
+    plan = sp.Plan(A, sp.default_opts())
+    info = plan.info
+    cb = int(info.compulsory_bytes)
+    assert cb == compulsory_bytes(n, m, nnz)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty(n, dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    launches_per_step = int(info.kernel_launches)
+
+    # correctness gate on the benchmark matrix: FP32 bound vs the high-precision oracle
+    sys.path.insert(0, str(ROOT / "tests"))
+    plan.run_device(xd.data_ptr(), yd.data_ptr(), sh)
+    torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        plan.run_device(xd.data_ptr(), yd.data_ptr(), sh)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(dev) as clk:
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            plan.run_device(xd.data_ptr(), yd.data_ptr(), sh)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    if world > 1:
+        dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    tot_ms = sum(ms)
+    if world > 1:
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    avg_ms = tot_ms / args.steps
+    gbs_rank = cb / (avg_ms * 1e-3) / 1e9
+    value = world * cb * args.steps / (tot_ms * 1e-3) / 1e9
+
+    # e2e through the C-ABI host path (pinned buffers, H2D x and D2H y per step)
+    hx = torch.from_numpy(x).pin_memory()
+    hy = torch.empty(n, dtype=torch.float32).pin_memory()
+    lib = sp.lib()
+    for _ in range(max(1, args.warmup)):
+        sp.capi.check(lib.sparsep_execute_host(plan.h, C.c_void_p(hx.data_ptr()), C.c_void_p(hy.data_ptr())))
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        sp.capi.check(lib.sparsep_execute_host(plan.h, C.c_void_p(hx.data_ptr()), C.c_void_p(hy.data_ptr())))
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    phases = plan.timings()
+    e2e_avg = sum(e2e_ms) / len(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_avg], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_avg = float(t.item())
+    y_dev = yd.cpu().numpy()
+    assert np.array_equal(y_dev, hy.numpy()), "device and host paths disagree"
+
+    peak, peak_kind = peaks()
+    traffic = None
+    tf = ROOT / "profiles" / "csr_f32_zipf1m_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+    res = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(avg_ms, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Zipf power-law matrix, numpy PCG64 seed 1)",
+        "config": {"workload": WORKLOAD, "nrows": n, "ncols": m, "nnz": nnz, "format": "csr",
+                   "scheme": "1d", "balance": "nnz (auto items)", "variant": info.variant.decode(),
+                   "items": int(info.items), "l2": "flushed (256 MB write) before every timed step",
+                   "compulsory_bytes_per_step": cb, "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(gbs_rank, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(gbs_rank / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": cb, "avg_launch_ms": round(avg_ms, 5)},
+        "e2e": {"value": round(cb / (e2e_avg * 1e-3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": m * 4,
+                "d2h_bytes_per_step": n * 4, "ms_per_step": round(e2e_avg, 4),
+                "phases_ms": {"load_input_vector": phases[1], "kernel": phases[2],
+                              "retrieve_output_vector": phases[3], "merge": phases[4],
+                              "load_matrix_once": phases[0]}},
+        "gpu_launches": launches_per_step * args.steps,
+        "gflops": round(2 * nnz / (avg_ms * 1e-3) / 1e9, 2),
+        "wall_s_timed_region": round(wall, 4),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_baseline(n, m, rowptr, colind, values, x, budget_s=args.cpu_budget,
+                                           threads=1)
+    plan.free()
+    return res
+
+
+def _ref_csr_lib():
+    so = ROOT / "oracle" / "_ref" / "libref_1D_CSR_row_f32.so"
+    if so.exists():
+        return C.CDLL(str(so)), "reference"
+    so = ROOT / "oracle" / "liboracle.so"
+    if not so.exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"], check=True)
+    return C.CDLL(str(so)), "port"
+
+
+def cpu_baseline(n, m, rowptr, colind, values, x, budget_s=15.0, threads=1):
+    """Time the reference's host CSR SpMV on a bounded number of full passes."""
+    import sparsep_b200 as sp
+
+    L, kind = _ref_csr_lib()
+    A = sp.csr("f32", n, m, rowptr, colind, values)
+    y = np.zeros(n + 8, np.float32)
+    xx = np.ascontiguousarray(x)
+    nnz = int(rowptr[-1])
+    cb = compulsory_bytes(n, m, nnz)
+
+    def one():
+        if threads == 1:
+            if kind == "reference":
+                L.ref_spmv(y.ctypes.data_as(C.c_void_p), A.ref, xx.ctypes.data_as(C.c_void_p))
+            else:
+                L.oracle_spmv_csr_f32(y.ctypes.data_as(C.c_void_p), A.ref, xx.ctypes.data_as(C.c_void_p))
+        else:
+            slices(L, kind, A, xx, y, threads)
+
+    t0 = time.perf_counter()
+    one()
+    first = time.perf_counter() - t0
+    reps = max(1, min(50, int(budget_s / max(first, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        one()
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": round(cb / dt / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"{reps} full SpMV passes over the {n}-row matrix ({nnz} nnz), {dt * 1e3:.1f} ms each",
+            "ms_per_spmv": round(dt * 1e3, 3), "cpu": _cpu_name()}
+
+
+def slices(L, kind, A, x, y, threads):
+    """Run the unchanged reference CSR loop on `threads` row slices in parallel."""
+    import concurrent.futures as cf
+
+    import sparsep_b200 as sp
+
+    s = A.s
+    n = int(s.nrows)
+    rp = A.arrays["rowptr"]
+    nnz = int(rp[n])
+    bounds = [0]
+    for t in range(1, threads):
+        bounds.append(int(np.searchsorted(rp[: n + 1], nnz * t // threads)))
+    bounds.append(n)
+    views = []
+    St = sp.capi.STRUCTS["f32"]["csr"]
+    for t in range(threads):
+        r0, r1 = bounds[t], bounds[t + 1]
+        v = St(r1 - r0, s.ncols, s.nnz, C.cast(C.addressof(s.rowptr.contents) + 4 * r0, sp.capi.P32),
+               s.colind, s.values)
+        views.append((v, r0))
+    fn = L.ref_spmv if kind == "reference" else L.oracle_spmv_csr_f32
+
+    def work(vr):
+        v, r0 = vr
+        fn(C.c_void_p(y.ctypes.data + 4 * r0), C.byref(v), x.ctypes.data_as(C.c_void_p))
+
+    with cf.ThreadPoolExecutor(threads) as ex:  # ctypes releases the GIL during the call
+        list(ex.map(work, views))
+
+
+def _cpu_name():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    n, m, rowptr, colind, values, x = make_matrix()
+    threads = os.cpu_count() or 1
+    L, kind = _ref_csr_lib()
+    import sparsep_b200 as sp
+
+    A = sp.csr("f32", n, m, rowptr, colind, values)
+    y = np.zeros(n + 8, np.float32)
+    nnz = int(rowptr[-1])
+    cb = compulsory_bytes(n, m, nnz)
+    for _ in range(args.warmup):
+        slices(L, kind, A, x, y, threads)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        slices(L, kind, A, x, y, threads)
+        ts.append(time.perf_counter() - t0)
+    avg = sum(ts) / len(ts)
+    v = round(cb / avg / 1e9, 3)
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(avg * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Zipf power-law matrix, numpy PCG64 seed 1)",
+            "config": {"workload": WORKLOAD, "nrows": n, "ncols": m, "nnz": nnz, "format": "csr", "scheme": "1d"},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} full SpMV passes, rows split over {threads} threads, "
+                                       "each slice running the reference's spmv_host loop",
+                             "cpu": _cpu_name()},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        if args.impl == "reference" and rank != 0:
+            return
+        if args.impl == "ours":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+    if world > 1 and args.impl == "ours":
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,493 @@
+/*
+ * sparsep.h -- C-ABI of sparsep_b200, a B200 (sm_100a) SpMV library.
+ *
+ * The library replaces the UPMEM segment of each SparseP host program
+ * (spmv/<1D|2D>/<kernel>/host/app.c: dpu_alloc .. dpu_push_xfer .. dpu_launch ..
+ * gather .. host merge) with one call over CUDA, while keeping the reference's
+ * matrix structs, .mtx reader, converters and partition/balance options.
+ *
+ * Every struct below is byte-compatible with the reference struct of the same
+ * role for the element type named by the suffix:
+ *     _i8 int8_t   _i16 int16_t   _i32 int32_t   _i64 int64_t   _f32 float   _f64 double
+ * (reference: spmv/1D/CSR-row/support/utils.h:12-34, `val_dt`).  Include
+ * "sparsep_compat.h" instead to get the reference's own names (struct CSRMatrix,
+ * val_dt, ...) selected by -DINT8 ... -DFP64 exactly as the reference does.
+ *
+ * Arithmetic contract (reference: spmv/1D/CSR-row/host/app.c:66-77):
+ *   y[r] = sum_j A[r][j] * x[j] with the sum taken in the element type.
+ *   Integer results wrap at the element width and are bit-exact against the
+ *   reference host SpMV for every format, scheme, balance and sync option.
+ *   FP32/FP64 results satisfy |dy_r| <= gamma_{n_r} * sum_j |A[r][j] x[j]|.
+ *
+ * Errors: every entry point returns an int status (0 = OK, negative errno-style
+ * code otherwise); nothing aborts.  Ownership: host structs stay owned by the
+ * caller; a plan owns its device copies.  A plan is not thread-safe; use one
+ * plan per host thread / stream.
+ */
+#ifndef SPARSEP_H_
+#define SPARSEP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define SPARSEP_OK 0
+#define SPARSEP_EIO (-5)         /* CUDA runtime error                        */
+#define SPARSEP_ENOMEM (-12)     /* host or device allocation failed          */
+#define SPARSEP_ENODEV (-19)     /* no CUDA device / kernel image not loadable*/
+#define SPARSEP_EINVAL (-22)     /* invalid argument, struct or option        */
+#define SPARSEP_ENOSYS (-38)     /* option combination not provided           */
+#define SPARSEP_ERANGE (-34)     /* size beyond a documented limit            */
+#define SPARSEP_ETIMEDOUT (-110) /* bounded device wait ran out               */
+#define SPARSEP_EBADF (-9)       /* .mtx file missing or malformed            */
+
+const char *sparsep_strerror(int status);
+
+/* ------------------------------------------------------------------------ */
+/* Element types (reference: -DINT8/INT16/INT32/INT64/FP32/FP64)             */
+/* ------------------------------------------------------------------------ */
+typedef enum {
+  SPARSEP_INT8 = 0,
+  SPARSEP_INT16 = 1,
+  SPARSEP_INT32 = 2,
+  SPARSEP_INT64 = 3,
+  SPARSEP_FP32 = 4,
+  SPARSEP_FP64 = 5
+} sparsep_dtype;
+
+/* ------------------------------------------------------------------------ */
+/* Options (reference: Makefile -D macros + getopt flags, see                 */
+/* spmv/1D/CSR-row/Makefile:4-8, spmv/1D/COO-nnz/Makefile:7-9,                */
+/* spmv/1D/BCSR-nnz/support/params.h:8-67, spmv/2D/BDCSR/support/params.h)    */
+/* ------------------------------------------------------------------------ */
+typedef enum {
+  SPARSEP_FMT_CSR = 0,
+  SPARSEP_FMT_COO = 1,
+  SPARSEP_FMT_BCSR = 2,
+  SPARSEP_FMT_BCOO = 3
+} sparsep_format;
+
+typedef enum {
+  SPARSEP_1D = 0,         /* row partitions, whole x per partition (spmv/1D)     */
+  SPARSEP_2D_EQUAL = 1,   /* D:   equal-sized tiles        (spmv/2D/D*)          */
+  SPARSEP_2D_EQUAL_W = 2, /* RBD: equal-width stripes x nnz-balanced row ranges */
+  SPARSEP_2D_VAR = 3      /* BD:  nnz-balanced stripes x nnz-balanced row ranges */
+} sparsep_scheme;
+
+typedef enum {
+  SPARSEP_BAL_ROW = 0,       /* equal rows (CSR-row, COO-row, partition_by_row)     */
+  SPARSEP_BAL_NNZ = 1,       /* equal nnz at row / block-row granularity            */
+  SPARSEP_BAL_BLOCK = 2,     /* equal blocks at block-row granularity (BCSR-block)  */
+  SPARSEP_BAL_NNZ_ELEM = 3,  /* equal nnz at element / block granularity; rows may
+                                straddle parts (COO-nnz, BCOO-nnz)                  */
+  SPARSEP_BAL_INTERLEAVE = 4 /* workers only: rows dealt round-robin to lane groups */
+} sparsep_balance;
+
+typedef enum {
+  SPARSEP_SYNC_LF = 0,     /* lock-free: partial sums merged without atomics (lf)  */
+  SPARSEP_SYNC_ATOMIC = 1, /* fine-grained: red.global per row segment (lb-fg)     */
+  SPARSEP_SYNC_CG = 2      /* coarse-grained lock (lb-cg); executed as ATOMIC       */
+} sparsep_sync;
+
+typedef struct sparsep_opts {
+  int32_t format;          /* sparsep_format (informational for typed entry points) */
+  int32_t scheme;          /* sparsep_scheme (informational for typed entry points) */
+  int32_t part_balance;    /* sparsep_balance across parts (reference: DPUs)     */
+  int32_t worker_balance;  /* sparsep_balance across workers (reference: tasklets)*/
+  int32_t sync;            /* sparsep_sync                                       */
+  int32_t nr_parts;        /* reference NR_DPUS: parts = CTAs; 0 = auto          */
+  int32_t nr_workers;      /* reference NR_TASKLETS: warps per part; 0 = auto    */
+  int32_t vert_partitions; /* reference -v (2D schemes built from COO)           */
+  int32_t row_block_size;  /* reference -r (BCSR/BCOO built from CSR)            */
+  int32_t col_block_size;  /* reference -c                                       */
+  int32_t lanes;           /* lanes per row / block row: 1,2,4,8,16,32; 0 = auto */
+  int32_t nrhs;            /* right-hand sides (x is ncols x nrhs row-major)     */
+  int32_t stage_x;         /* 2D: stage the x-segment in shared memory (1/0/-1=auto) */
+  int32_t reserved[3];
+} sparsep_opts;
+
+/* Defaults: 1D, nnz balance, auto parts/workers/lanes, LF, nrhs = 1. */
+void sparsep_opts_default(sparsep_opts *o);
+
+/* ------------------------------------------------------------------------ */
+/* Reference structs, byte-compatible per element type                       */
+/* ------------------------------------------------------------------------ */
+/* spmv/1D/BCOO-nnz/support/utils.h:39-42 */
+typedef struct sparsep_bind {
+  uint32_t rowind;
+  uint32_t colind;
+} sparsep_bind;
+
+#define SPARSEP_DEFINE_TYPES(T, S)                                                  \
+  /* AoS nonzero, spmv/1D/COO-nnz/support/utils.h:39-43 */                          \
+  typedef struct sparsep_elem_##S {                                                 \
+    uint32_t rowind;                                                                \
+    uint32_t colind;                                                                \
+    T val;                                                                          \
+  } sparsep_elem_##S;                                                               \
+  /* SoA COO, spmv/1D/CSR-row/support/matrix.h:19-26 */                             \
+  typedef struct sparsep_coo_##S {                                                  \
+    uint32_t nrows, ncols, nnz;                                                     \
+    uint32_t *rowindx;                                                              \
+    uint32_t *colind;                                                               \
+    T *values;                                                                      \
+  } sparsep_coo_##S;                                                                \
+  /* AoS COO with per-row counts, spmv/1D/COO-nnz/support/matrix.h:19-25 */         \
+  typedef struct sparsep_cooe_##S {                                                 \
+    uint32_t nrows, ncols, nnz;                                                     \
+    uint32_t *rows;                                                                 \
+    sparsep_elem_##S *nnzs;                                                         \
+  } sparsep_cooe_##S;                                                               \
+  /* spmv/1D/CSR-row/support/matrix.h:31-38 */                                      \
+  typedef struct sparsep_csr_##S {                                                  \
+    uint32_t nrows, ncols, nnz;                                                     \
+    uint32_t *rowptr;                                                               \
+    uint32_t *colind;                                                               \
+    T *values;                                                                      \
+  } sparsep_csr_##S;                                                                \
+  /* spmv/1D/BCSR-nnz/support/matrix.h:43-57 */                                     \
+  typedef struct sparsep_bcsr_##S {                                                 \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols;                                        \
+    uint64_t num_blocks;                                                            \
+    uint32_t num_rows_left, nrows, ncols, nnz;                                      \
+    uint32_t *browptr;                                                              \
+    uint32_t *bcolind;                                                              \
+    T *bval;                                                                        \
+    uint32_t *nnz_per_block;                                                        \
+  } sparsep_bcsr_##S;                                                               \
+  /* spmv/1D/BCOO-nnz/support/matrix.h:62-76 */                                     \
+  typedef struct sparsep_bcoo_##S {                                                 \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols;                                        \
+    uint64_t num_blocks;                                                            \
+    uint32_t num_rows_left, nrows, ncols, nnz;                                      \
+    sparsep_bind *bind;                                                             \
+    T *bval;                                                                        \
+    uint32_t *nnz_per_block;                                                        \
+  } sparsep_bcoo_##S;                                                               \
+  /* spmv/2D/DCSR/support/matrix.h:31-44 */                                         \
+  typedef struct sparsep_dcsr_##S {                                                 \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t tile_height, tile_width;                                               \
+    uint32_t *nnzs_per_partition;                                                   \
+    uint32_t *drowptr;                                                              \
+    uint32_t *dcolind;                                                              \
+    T *dval;                                                                        \
+  } sparsep_dcsr_##S;                                                               \
+  /* spmv/2D/RBDCSR/support/matrix.h:31-43 */                                       \
+  typedef struct sparsep_rbdcsr_##S {                                               \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t tile_width;                                                            \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *drowptr;                                                              \
+    uint32_t *dcolind;                                                              \
+    T *dval;                                                                        \
+  } sparsep_rbdcsr_##S;                                                             \
+  /* spmv/2D/BDCSR/support/matrix.h:31-45 */                                        \
+  typedef struct sparsep_bdcsr_##S {                                                \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t max_tile_width;                                                        \
+    uint32_t *vert_tile_widths;                                                     \
+    uint32_t *nnzs_per_column;                                                      \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *drowptr;                                                              \
+    uint32_t *dcolind;                                                              \
+    T *dval;                                                                        \
+  } sparsep_bdcsr_##S;                                                              \
+  /* spmv/2D/DCOO/support/matrix.h:30-42 */                                         \
+  typedef struct sparsep_dcoo_##S {                                                 \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t tile_height, tile_width;                                               \
+    uint32_t *nnzs_per_partition;                                                   \
+    sparsep_elem_##S *nnzs;                                                         \
+  } sparsep_dcoo_##S;                                                               \
+  /* spmv/2D/RBDCOO/support/matrix.h:31 */                                          \
+  typedef struct sparsep_rbdcoo_##S {                                               \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t tile_width;                                                            \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    sparsep_elem_##S *nnzs;                                                         \
+  } sparsep_rbdcoo_##S;                                                             \
+  /* spmv/2D/BDCOO/support/matrix.h:30 */                                           \
+  typedef struct sparsep_bdcoo_##S {                                                \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t max_tile_width;                                                        \
+    uint32_t *vert_tile_widths;                                                     \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *nnzs_per_column;                                                      \
+    sparsep_elem_##S *nnzs;                                                         \
+  } sparsep_bdcoo_##S;                                                              \
+  /* spmv/2D/DBCSR/support/matrix.h:50-71 */                                        \
+  typedef struct sparsep_dbcsr_##S {                                                \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t nblocks;                                                               \
+    uint64_t tile_height, tile_width;                                               \
+    uint32_t *nnzs_per_partition;                                                   \
+    uint32_t *blocks_per_partition;                                                 \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols, num_rows_left;                         \
+    uint32_t *browptr;                                                              \
+    uint32_t *bcolind;                                                              \
+    T *bval;                                                                        \
+    uint32_t *nnz_per_block;                                                        \
+  } sparsep_dbcsr_##S;                                                              \
+  /* spmv/2D/DBCOO/support/matrix.h:77 */                                           \
+  typedef struct sparsep_dbcoo_##S {                                                \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t nblocks;                                                               \
+    uint64_t tile_height, tile_width;                                               \
+    uint32_t *nnzs_per_partition;                                                   \
+    uint32_t *blocks_per_partition;                                                 \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols, num_rows_left;                         \
+    sparsep_bind *bind;                                                             \
+    T *bval;                                                                        \
+    uint32_t *nnz_per_block;                                                        \
+  } sparsep_dbcoo_##S;                                                              \
+  /* spmv/2D/RBDBCSR-nnz/support/matrix.h:50 */                                     \
+  typedef struct sparsep_rbdbcsr_##S {                                              \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t nblocks;                                                               \
+    uint32_t tile_width;                                                            \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *blocks_per_vert_partition;                                            \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols, num_rows_left;                         \
+    uint32_t *browptr;                                                              \
+    uint32_t *bcolind;                                                              \
+    T *bval;                                                                        \
+    uint32_t *nnz_per_block;                                                        \
+  } sparsep_rbdbcsr_##S;                                                            \
+  /* spmv/2D/RBDBCOO-nnz/support/matrix.h:76 */                                     \
+  typedef struct sparsep_rbdbcoo_##S {                                              \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t nblocks;                                                               \
+    uint32_t tile_width;                                                            \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *blocks_per_vert_partition;                                            \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols, num_rows_left;                         \
+    sparsep_bind *bind;                                                             \
+    T *bval;                                                                        \
+    uint32_t *nnz_per_block;                                                        \
+  } sparsep_rbdbcoo_##S;                                                            \
+  /* spmv/2D/BDBCSR-nnz/support/matrix.h:51 */                                      \
+  typedef struct sparsep_bdbcsr_##S {                                               \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t nblocks;                                                               \
+    uint32_t max_tile_width;                                                        \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *nnzs_per_column;                                                      \
+    uint32_t *blocks_per_vert_partition;                                            \
+    uint32_t *vert_tile_widths;                                                     \
+    uint32_t *nnz_per_block;                                                        \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols, num_rows_left;                         \
+    uint32_t *browptr;                                                              \
+    uint32_t *bcolind;                                                              \
+    T *bval;                                                                        \
+  } sparsep_bdbcsr_##S;                                                             \
+  /* spmv/2D/BDBCOO-nnz/support/matrix.h:79 */                                      \
+  typedef struct sparsep_bdbcoo_##S {                                               \
+    uint32_t nrows, ncols, nnz, npartitions, horz_partitions, vert_partitions;      \
+    uint32_t nblocks;                                                               \
+    uint32_t max_tile_width;                                                        \
+    uint32_t *nnzs_per_column;                                                      \
+    uint32_t *nnzs_per_vert_partition;                                              \
+    uint32_t *blocks_per_vert_partition;                                            \
+    uint32_t *vert_tile_widths;                                                     \
+    uint32_t *nnz_per_block;                                                        \
+    uint64_t row_block_size, col_block_size;                                        \
+    uint32_t num_block_rows, num_block_cols, num_rows_left;                         \
+    sparsep_bind *bind;                                                             \
+    T *bval;                                                                        \
+  } sparsep_bdbcoo_##S;
+
+SPARSEP_DEFINE_TYPES(int8_t, i8)
+SPARSEP_DEFINE_TYPES(int16_t, i16)
+SPARSEP_DEFINE_TYPES(int32_t, i32)
+SPARSEP_DEFINE_TYPES(int64_t, i64)
+SPARSEP_DEFINE_TYPES(float, f32)
+SPARSEP_DEFINE_TYPES(double, f64)
+
+/* ------------------------------------------------------------------------ */
+/* Plans: the reference's Load Matrix phase done once, executed many times  */
+/* ------------------------------------------------------------------------ */
+typedef struct sparsep_plan sparsep_plan;
+
+/* Reference timer slots (spmv/1D/CSR-row/host/app.c:291-300), milliseconds of
+ * the most recent call: 0 Load Matrix, 1 Load Input Vector, 2 Kernel,
+ * 3 Retrieve Output Vector, 4 Merge Partial Results. */
+int sparsep_timings(const sparsep_plan *plan, double ms[5]);
+
+typedef struct sparsep_plan_info {
+  int32_t dtype, format, scheme, nrhs;
+  uint32_t nrows, ncols;
+  uint64_t nnz;           /* stored nonzeros (blocks: stored entries)          */
+  uint64_t nblocks;       /* BCSR/BCOO                                          */
+  uint64_t items;         /* CTA work items per execution                      */
+  uint64_t tiles;         /* tiles (parts) per execution                       */
+  uint64_t compulsory_bytes; /* bytes one SpMV must move (values, indices, x, y) */
+  uint64_t device_bytes;  /* device memory held by the plan                    */
+  uint64_t scratch_bytes; /* of which scratch (partials, carries, counters)   */
+  int32_t kernel_launches; /* kernels launched per execution                   */
+  int32_t lanes, workers, stage_x;
+  char variant[96];       /* human-readable variant name                      */
+} sparsep_plan_info;
+
+int sparsep_plan_get_info(const sparsep_plan *plan, sparsep_plan_info *info);
+void sparsep_plan_free(sparsep_plan *plan);
+
+/* Execute with DEVICE pointers on a CUDA stream (cudaStream_t as void*, NULL =
+ * legacy default stream).  x holds ncols*nrhs elements, y receives nrows*nrhs.
+ * Stream-ordered; nothing synchronises.  Safe for CUDA graph capture after the
+ * first call on that plan. */
+int sparsep_execute_device(sparsep_plan *plan, const void *d_x, void *d_y, void *stream);
+
+/* Execute with HOST pointers: H2D x, kernel(s), D2H y, synchronous.  Fills the
+ * timer slots 1..4. */
+int sparsep_execute_host(sparsep_plan *plan, const void *h_x, void *h_y);
+
+/* Device-resident x / y buffers owned by the plan (ncols*nrhs, nrows*nrhs). */
+void *sparsep_plan_x(sparsep_plan *plan);
+void *sparsep_plan_y(sparsep_plan *plan);
+
+/* ------------------------------------------------------------------------ */
+/* Per-dtype entry points                                                    */
+/* ------------------------------------------------------------------------ */
+/* For each struct kind K in {csr, coo, cooe, bcsr, bcoo, dcsr, rbdcsr, bdcsr,
+ * dcoo, rbdcoo, bdcoo, dbcsr, dbcoo, rbdbcsr, rbdbcoo, bdbcsr, bdbcoo}:
+ *   sparsep_plan_K_S(const sparsep_K_S *A, const sparsep_opts *o, sparsep_plan **out)
+ *   sparsep_spmv_K_S(const sparsep_K_S *A, const T *x, T *y, const sparsep_opts *o)
+ * The one-shot form plans, executes on host buffers and frees (the whole
+ * reference main() between reading the matrix and printing the timers).
+ *
+ * Lengths: x has ncols elements (BCSR/BCOO: ncols; 2D: ncols), y has nrows
+ * elements; entries of y past nrows are never written.  cooe / 2D COO inputs
+ * must be sorted by (row, col) as the reference's sortCOOMatrix leaves them
+ * (spmv/1D/COO-nnz/support/matrix.h:88-125); 2D tiles as the reference
+ * converters produce them.
+ *
+ * Readers and converters (host, reference support/matrix.h semantics):
+ *   sparsep_read_coo_S(file, &coo)      readCOOMatrix, SoA, pads nrows/ncols to 8/sizeof(T)
+ *                                       (spmv/1D/CSR-row/support/matrix.h:44-96)
+ *   sparsep_read_coo_nopad_S(file, &coo) same without padding (spmv/1D/BCSR-nnz/support/matrix.h:63-110)
+ *   sparsep_read_cooe_S(file, &cooe)    readCOOMatrix, AoS (spmv/1D/COO-nnz/support/matrix.h:31-83)
+ *   sparsep_sort_cooe_S(cooe)           sortCOOMatrix (spmv/1D/COO-nnz/support/matrix.h:88-125)
+ *   sparsep_coo2csr_S(coo, &csr)        coo2csr (spmv/1D/CSR-row/support/matrix.h:113-152)
+ *   sparsep_csr2bcsr_S(csr, rb, cb, &b) csr2bcsr + sortBCSRMatrix + countNNZperBlockBCSRMatrix
+ *                                       (spmv/1D/BCSR-nnz/support/matrix.h:202-485)
+ *   sparsep_bcsr2bcoo_S(bcsr, &bcoo)    bcsr2bcoo (spmv/1D/BCOO-nnz/support/matrix.h:549-578)
+ *   sparsep_cooe2dcsr_S(cooe, H, V, &d)   coo2dcsr   (spmv/2D/DCSR/support/matrix.h:159-230)
+ *   sparsep_cooe2rbdcsr_S(cooe, H, V, &d) coo2rbdcsr (spmv/2D/RBDCSR/support/matrix.h:159-223)
+ *   sparsep_cooe2bdcsr_S(cooe, H, V, &d)  coo2bdcsr  (spmv/2D/BDCSR/support/matrix.h:161-282)
+ *   sparsep_cooe2dcoo_S / rbdcoo / bdcoo  coo2dcoo etc. (spmv/2D/DCOO/support/matrix.h:158-217)
+ *   sparsep_dcsr2dbcsr_S(d, rb, cb, &b)   dcsr2dbcsr + countNNZperBlock (spmv/2D/DBCSR/support/matrix.h:278-557)
+ *   sparsep_dcsr2dbcoo_S, sparsep_rbdcsr2rbdbcsr_S, sparsep_rbdcsr2rbdbcoo_S,
+ *   sparsep_bdcsr2bdbcsr_S, sparsep_bdcsr2bdbcoo_S   (the other 2D block converters)
+ *   sparsep_free_K_S(ptr)               frees a struct returned by the library
+ */
+#define SPARSEP_DECLARE_KIND(T, S, K)                                                    \
+  int sparsep_plan_##K##_##S(const sparsep_##K##_##S *A, const sparsep_opts *o,          \
+                             sparsep_plan **out);                                        \
+  int sparsep_spmv_##K##_##S(const sparsep_##K##_##S *A, const T *x, T *y,               \
+                             const sparsep_opts *o);                                     \
+  void sparsep_free_##K##_##S(sparsep_##K##_##S *A);
+
+#define SPARSEP_DECLARE_DTYPE(T, S)                                                      \
+  SPARSEP_DECLARE_KIND(T, S, csr)                                                        \
+  SPARSEP_DECLARE_KIND(T, S, coo)                                                        \
+  SPARSEP_DECLARE_KIND(T, S, cooe)                                                       \
+  SPARSEP_DECLARE_KIND(T, S, bcsr)                                                       \
+  SPARSEP_DECLARE_KIND(T, S, bcoo)                                                       \
+  SPARSEP_DECLARE_KIND(T, S, dcsr)                                                       \
+  SPARSEP_DECLARE_KIND(T, S, rbdcsr)                                                     \
+  SPARSEP_DECLARE_KIND(T, S, bdcsr)                                                      \
+  SPARSEP_DECLARE_KIND(T, S, dcoo)                                                       \
+  SPARSEP_DECLARE_KIND(T, S, rbdcoo)                                                     \
+  SPARSEP_DECLARE_KIND(T, S, bdcoo)                                                      \
+  SPARSEP_DECLARE_KIND(T, S, dbcsr)                                                      \
+  SPARSEP_DECLARE_KIND(T, S, dbcoo)                                                      \
+  SPARSEP_DECLARE_KIND(T, S, rbdbcsr)                                                    \
+  SPARSEP_DECLARE_KIND(T, S, rbdbcoo)                                                    \
+  SPARSEP_DECLARE_KIND(T, S, bdbcsr)                                                     \
+  SPARSEP_DECLARE_KIND(T, S, bdbcoo)                                                     \
+  int sparsep_read_coo_##S(const char *file, sparsep_coo_##S **out);                     \
+  int sparsep_read_coo_nopad_##S(const char *file, sparsep_coo_##S **out);               \
+  int sparsep_read_cooe_##S(const char *file, sparsep_cooe_##S **out);                   \
+  int sparsep_sort_cooe_##S(sparsep_cooe_##S *A);                                        \
+  int sparsep_coo2csr_##S(const sparsep_coo_##S *A, sparsep_csr_##S **out);              \
+  int sparsep_csr2bcsr_##S(const sparsep_csr_##S *A, uint32_t rb, uint32_t cb,           \
+                           sparsep_bcsr_##S **out);                                      \
+  int sparsep_bcsr2bcoo_##S(const sparsep_bcsr_##S *A, sparsep_bcoo_##S **out);          \
+  int sparsep_cooe2dcsr_##S(const sparsep_cooe_##S *A, uint32_t h, uint32_t v,           \
+                            sparsep_dcsr_##S **out);                                     \
+  int sparsep_cooe2rbdcsr_##S(const sparsep_cooe_##S *A, uint32_t h, uint32_t v,         \
+                              sparsep_rbdcsr_##S **out);                                 \
+  int sparsep_cooe2bdcsr_##S(const sparsep_cooe_##S *A, uint32_t h, uint32_t v,          \
+                             sparsep_bdcsr_##S **out);                                   \
+  int sparsep_cooe2dcoo_##S(const sparsep_cooe_##S *A, uint32_t h, uint32_t v,           \
+                            sparsep_dcoo_##S **out);                                     \
+  int sparsep_cooe2rbdcoo_##S(const sparsep_cooe_##S *A, uint32_t h, uint32_t v,         \
+                              sparsep_rbdcoo_##S **out);                                 \
+  int sparsep_cooe2bdcoo_##S(const sparsep_cooe_##S *A, uint32_t h, uint32_t v,          \
+                             sparsep_bdcoo_##S **out);                                   \
+  int sparsep_dcsr2dbcsr_##S(const sparsep_dcsr_##S *A, uint32_t rb, uint32_t cb,        \
+                             sparsep_dbcsr_##S **out);                                   \
+  int sparsep_dcsr2dbcoo_##S(const sparsep_dcsr_##S *A, uint32_t rb, uint32_t cb,        \
+                             sparsep_dbcoo_##S **out);                                   \
+  int sparsep_rbdcsr2rbdbcsr_##S(const sparsep_rbdcsr_##S *A, uint32_t rb, uint32_t cb,  \
+                                 sparsep_rbdbcsr_##S **out);                             \
+  int sparsep_rbdcsr2rbdbcoo_##S(const sparsep_rbdcsr_##S *A, uint32_t rb, uint32_t cb,  \
+                                 sparsep_rbdbcoo_##S **out);                             \
+  int sparsep_bdcsr2bdbcsr_##S(const sparsep_bdcsr_##S *A, uint32_t rb, uint32_t cb,     \
+                               sparsep_bdbcsr_##S **out);                                \
+  int sparsep_bdcsr2bdbcoo_##S(const sparsep_bdcsr_##S *A, uint32_t rb, uint32_t cb,     \
+                               sparsep_bdbcoo_##S **out);
+
+SPARSEP_DECLARE_DTYPE(int8_t, i8)
+SPARSEP_DECLARE_DTYPE(int16_t, i16)
+SPARSEP_DECLARE_DTYPE(int32_t, i32)
+SPARSEP_DECLARE_DTYPE(int64_t, i64)
+SPARSEP_DECLARE_DTYPE(float, f32)
+SPARSEP_DECLARE_DTYPE(double, f64)
+
+/* ------------------------------------------------------------------------ */
+/* Partitioners (reference semantics, host).  `split` receives parts+1      */
+/* boundaries.  Exposed so callers can reproduce the reference's DPU split; */
+/* the plans use the same code for nr_parts > 0.                            */
+/* ------------------------------------------------------------------------ */
+/* partition_by_row, spmv/1D/CSR-row/support/partition.h:35-60 */
+int sparsep_partition_by_row(uint32_t nrows, uint32_t parts, uint32_t *split);
+/* partition_by_nnz (row granularity), spmv/1D/CSR-nnz/support/partition.h:35-77 */
+int sparsep_partition_by_nnz(const uint32_t *rowptr, uint32_t nrows, uint32_t parts,
+                             uint32_t *split);
+/* element-granular equal-nnz split, spmv/1D/COO-nnz/host/app.c:118-156:
+ * split[i] = first nnz of part i (rows may straddle parts). */
+int sparsep_partition_by_elem(uint64_t nnz, uint32_t parts, uint64_t *split);
+/* BCSR partition_by_nnz / partition_by_blocks at block-row granularity,
+ * spmv/1D/BCSR-nnz/support/partition.h:39-112, spmv/1D/BCSR-block/support/partition.h:39.
+ * weights[b] = nnz_per_block[b] (by nnz) or NULL (by blocks). */
+int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_rows,
+                                 const uint32_t *weights, uint32_t parts, uint32_t *split);
+
+/* ------------------------------------------------------------------------ */
+/* Device information                                                        */
+/* ------------------------------------------------------------------------ */
+/* Number of SMs of the current device, or a negative status. */
+int sparsep_device_sms(void);
+/* Library version string. */
+const char *sparsep_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARSEP_H_ */

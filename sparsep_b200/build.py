@@ -1,0 +1,85 @@
+"""Build libsparsep_b200.so in-tree with nvcc for sm_100a.
+
+Sources: csrc/kernels.cu (compiled once per element type, in parallel),
+csrc/plan.cu and csrc/formats.cpp.  Objects go to sparsep_b200/_build/.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libsparsep_b200.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+              f"-I{ROOT / 'include'}", f"-I{CSRC}"]
+KERNEL_TYPES = {"i8": "int8_t", "i16": "int16_t", "i32": "int32_t", "i64": "int64_t",
+                "f32": "float", "f64": "double"}
+
+
+def nvcc() -> str:
+    p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(p).exists():
+        raise RuntimeError("nvcc not found")
+    return p
+
+
+def _sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")) + list(CSRC.glob("*.cuh"))
+                  + list(CSRC.glob("*.hpp")) + [ROOT / "include" / "sparsep.h"])
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    deps = _sources()
+    if not force and not _stale(LIB, deps):
+        return LIB
+    jobs = []
+    objs = []
+    for tag, ctype in KERNEL_TYPES.items():
+        o = BUILD / f"kernels_{tag}.o"
+        objs.append(o)
+        jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / "kernels.cu"),
+                     "-o", str(o)])
+    for src in sorted(CSRC.glob("*.cu")):
+        if src.name == "kernels.cu":
+            continue
+        o = BUILD / (src.stem + ".o")
+        objs.append(o)
+        jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(o)])
+    for src in sorted(CSRC.glob("*.cpp")):
+        o = BUILD / (src.stem + ".o")
+        objs.append(o)
+        jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, "-x", "cu", "-c", str(src), "-o", str(o)])
+    with cf.ThreadPoolExecutor(max_workers=max(2, os.cpu_count() or 2)) as ex:
+        list(ex.map(_run, jobs))
+    tmp = LIB.with_suffix(".so.tmp")
+    _run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
+    os.replace(tmp, LIB)
+    if verbose:
+        print(f"built {LIB}")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

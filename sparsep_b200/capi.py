@@ -1,0 +1,375 @@
+"""ctypes binding of the sparsep_b200 C-ABI (include/sparsep.h).
+
+This is the host-side mirror of the reference's interface for Python callers
+(tests, bench, autotuner): the reference's matrix structs as ctypes structures
+per element type, builders from numpy arrays, and a Plan object over
+sparsep_plan.  The compute path is always libsparsep_b200.so; importing this
+module raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libsparsep_b200.so"
+
+# status codes
+OK, EIO, ENOMEM, ENODEV, EINVAL, ENOSYS, ERANGE, ETIMEDOUT, EBADF = 0, -5, -12, -19, -22, -38, -34, -110, -9
+FMT_CSR, FMT_COO, FMT_BCSR, FMT_BCOO = range(4)
+S1D, S2D_EQUAL, S2D_EQUAL_W, S2D_VAR = range(4)
+BAL_ROW, BAL_NNZ, BAL_BLOCK, BAL_NNZ_ELEM, BAL_INTERLEAVE = range(5)
+SYNC_LF, SYNC_ATOMIC, SYNC_CG = range(3)
+
+
+@dataclass(frozen=True)
+class DType:
+    name: str       # suffix in the C-ABI (i8 ... f64)
+    code: int       # sparsep_dtype
+    np: Any         # numpy dtype
+    ct: Any         # ctypes scalar
+    macro: str      # reference -D macro
+
+
+DTYPES = {
+    "i8": DType("i8", 0, np.int8, C.c_int8, "INT8"),
+    "i16": DType("i16", 1, np.int16, C.c_int16, "INT16"),
+    "i32": DType("i32", 2, np.int32, C.c_int32, "INT32"),
+    "i64": DType("i64", 3, np.int64, C.c_int64, "INT64"),
+    "f32": DType("f32", 4, np.float32, C.c_float, "FP32"),
+    "f64": DType("f64", 5, np.float64, C.c_double, "FP64"),
+}
+
+P32 = C.POINTER(C.c_uint32)
+
+
+class Bind(C.Structure):
+    _fields_ = [("rowind", C.c_uint32), ("colind", C.c_uint32)]
+
+
+class Opts(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "format", "scheme", "part_balance", "worker_balance", "sync", "nr_parts", "nr_workers",
+        "vert_partitions", "row_block_size", "col_block_size", "lanes", "nrhs", "stage_x")] + [
+        ("reserved", C.c_int32 * 3)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("dtype", C.c_int32), ("format", C.c_int32), ("scheme", C.c_int32), ("nrhs", C.c_int32),
+                ("nrows", C.c_uint32), ("ncols", C.c_uint32), ("nnz", C.c_uint64), ("nblocks", C.c_uint64),
+                ("items", C.c_uint64), ("tiles", C.c_uint64), ("compulsory_bytes", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("scratch_bytes", C.c_uint64), ("kernel_launches", C.c_int32),
+                ("lanes", C.c_int32), ("workers", C.c_int32), ("stage_x", C.c_int32), ("variant", C.c_char * 96)]
+
+
+def _struct_types(dt: DType) -> dict[str, type]:
+    T = dt.ct
+    PT = C.POINTER(T)
+
+    class Elem(C.Structure):
+        _fields_ = [("rowind", C.c_uint32), ("colind", C.c_uint32), ("val", T)]
+
+    PE = C.POINTER(Elem)
+    PB = C.POINTER(Bind)
+    u32 = C.c_uint32
+    u64 = C.c_uint64
+
+    def mk(name, fields):
+        return type(f"{name}_{dt.name}", (C.Structure,), {"_fields_": fields})
+
+    d: dict[str, type] = {"elem": Elem}
+    d["coo"] = mk("coo", [("nrows", u32), ("ncols", u32), ("nnz", u32), ("rowindx", P32), ("colind", P32),
+                          ("values", PT)])
+    d["cooe"] = mk("cooe", [("nrows", u32), ("ncols", u32), ("nnz", u32), ("rows", P32), ("nnzs", PE)])
+    d["csr"] = mk("csr", [("nrows", u32), ("ncols", u32), ("nnz", u32), ("rowptr", P32), ("colind", P32),
+                          ("values", PT)])
+    blk = [("row_block_size", u64), ("col_block_size", u64), ("num_block_rows", u32), ("num_block_cols", u32),
+           ("num_blocks", u64), ("num_rows_left", u32), ("nrows", u32), ("ncols", u32), ("nnz", u32)]
+    d["bcsr"] = mk("bcsr", blk + [("browptr", P32), ("bcolind", P32), ("bval", PT), ("nnz_per_block", P32)])
+    d["bcoo"] = mk("bcoo", blk + [("bind", PB), ("bval", PT), ("nnz_per_block", P32)])
+    hd = [("nrows", u32), ("ncols", u32), ("nnz", u32), ("npartitions", u32), ("horz_partitions", u32),
+          ("vert_partitions", u32)]
+    d["dcsr"] = mk("dcsr", hd + [("tile_height", u32), ("tile_width", u32), ("nnzs_per_partition", P32),
+                                 ("drowptr", P32), ("dcolind", P32), ("dval", PT)])
+    d["rbdcsr"] = mk("rbdcsr", hd + [("tile_width", u32), ("nnzs_per_vert_partition", P32), ("drowptr", P32),
+                                     ("dcolind", P32), ("dval", PT)])
+    d["bdcsr"] = mk("bdcsr", hd + [("max_tile_width", u32), ("vert_tile_widths", P32), ("nnzs_per_column", P32),
+                                   ("nnzs_per_vert_partition", P32), ("drowptr", P32), ("dcolind", P32),
+                                   ("dval", PT)])
+    d["dcoo"] = mk("dcoo", hd + [("tile_height", u32), ("tile_width", u32), ("nnzs_per_partition", P32),
+                                 ("nnzs", PE)])
+    d["rbdcoo"] = mk("rbdcoo", hd + [("tile_width", u32), ("nnzs_per_vert_partition", P32), ("nnzs", PE)])
+    d["bdcoo"] = mk("bdcoo", hd + [("max_tile_width", u32), ("vert_tile_widths", P32),
+                                   ("nnzs_per_vert_partition", P32), ("nnzs_per_column", P32), ("nnzs", PE)])
+    geo = [("row_block_size", u64), ("col_block_size", u64), ("num_block_rows", u32), ("num_block_cols", u32),
+           ("num_rows_left", u32)]
+    d["dbcsr"] = mk("dbcsr", hd + [("nblocks", u32), ("tile_height", u64), ("tile_width", u64),
+                                   ("nnzs_per_partition", P32), ("blocks_per_partition", P32)] + geo +
+                    [("browptr", P32), ("bcolind", P32), ("bval", PT), ("nnz_per_block", P32)])
+    d["dbcoo"] = mk("dbcoo", hd + [("nblocks", u32), ("tile_height", u64), ("tile_width", u64),
+                                   ("nnzs_per_partition", P32), ("blocks_per_partition", P32)] + geo +
+                    [("bind", PB), ("bval", PT), ("nnz_per_block", P32)])
+    d["rbdbcsr"] = mk("rbdbcsr", hd + [("nblocks", u32), ("tile_width", u32), ("nnzs_per_vert_partition", P32),
+                                       ("blocks_per_vert_partition", P32)] + geo +
+                      [("browptr", P32), ("bcolind", P32), ("bval", PT), ("nnz_per_block", P32)])
+    d["rbdbcoo"] = mk("rbdbcoo", hd + [("nblocks", u32), ("tile_width", u32), ("nnzs_per_vert_partition", P32),
+                                       ("blocks_per_vert_partition", P32)] + geo +
+                      [("bind", PB), ("bval", PT), ("nnz_per_block", P32)])
+    d["bdbcsr"] = mk("bdbcsr", hd + [("nblocks", u32), ("max_tile_width", u32), ("nnzs_per_vert_partition", P32),
+                                     ("nnzs_per_column", P32), ("blocks_per_vert_partition", P32),
+                                     ("vert_tile_widths", P32), ("nnz_per_block", P32)] + geo +
+                     [("browptr", P32), ("bcolind", P32), ("bval", PT)])
+    d["bdbcoo"] = mk("bdbcoo", hd + [("nblocks", u32), ("max_tile_width", u32), ("nnzs_per_column", P32),
+                                     ("nnzs_per_vert_partition", P32), ("blocks_per_vert_partition", P32),
+                                     ("vert_tile_widths", P32), ("nnz_per_block", P32)] + geo +
+                     [("bind", PB), ("bval", PT)])
+    return d
+
+
+STRUCTS = {k: _struct_types(v) for k, v in DTYPES.items()}
+KINDS = ["csr", "coo", "cooe", "bcsr", "bcoo", "dcsr", "rbdcsr", "bdcsr", "dcoo", "rbdcoo", "bdcoo", "dbcsr",
+         "dbcoo", "rbdbcsr", "rbdbcoo", "bdbcsr", "bdbcoo"]
+CONVERTERS = {  # name: (input kind, output kind, extra uint32 args)
+    "coo2csr": ("coo", "csr", 0), "csr2bcsr": ("csr", "bcsr", 2), "bcsr2bcoo": ("bcsr", "bcoo", 0),
+    "cooe2dcsr": ("cooe", "dcsr", 2), "cooe2rbdcsr": ("cooe", "rbdcsr", 2), "cooe2bdcsr": ("cooe", "bdcsr", 2),
+    "cooe2dcoo": ("cooe", "dcoo", 2), "cooe2rbdcoo": ("cooe", "rbdcoo", 2), "cooe2bdcoo": ("cooe", "bdcoo", 2),
+    "dcsr2dbcsr": ("dcsr", "dbcsr", 2), "dcsr2dbcoo": ("dcsr", "dbcoo", 2),
+    "rbdcsr2rbdbcsr": ("rbdcsr", "rbdbcsr", 2), "rbdcsr2rbdbcoo": ("rbdcsr", "rbdbcoo", 2),
+    "bdcsr2bdbcsr": ("bdcsr", "bdbcsr", 2), "bdcsr2bdbcoo": ("bdcsr", "bdbcoo", 2),
+}
+
+_lib: C.CDLL | None = None
+
+
+class SparsepError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = lib().sparsep_strerror(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} ({status})" if what else f"{msg} ({status})")
+
+
+def check(st: int, what: str = "") -> None:
+    if st != OK:
+        raise SparsepError(st, what)
+
+
+def lib() -> C.CDLL:
+    """Load libsparsep_b200.so (in-tree).  No fallback: a missing library is an error."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m sparsep_b200.build` "
+                          "(the CUDA path has no CPU fallback)")
+    L = C.CDLL(str(LIB_PATH))
+    L.sparsep_strerror.restype = C.c_char_p
+    L.sparsep_version.restype = C.c_char_p
+    L.sparsep_opts_default.argtypes = [C.POINTER(Opts)]
+    L.sparsep_plan_free.argtypes = [C.c_void_p]
+    L.sparsep_plan_get_info.argtypes = [C.c_void_p, C.POINTER(PlanInfo)]
+    L.sparsep_timings.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.sparsep_execute_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sparsep_execute_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sparsep_plan_x.argtypes = [C.c_void_p]
+    L.sparsep_plan_x.restype = C.c_void_p
+    L.sparsep_plan_y.argtypes = [C.c_void_p]
+    L.sparsep_plan_y.restype = C.c_void_p
+    L.sparsep_partition_by_row.argtypes = [C.c_uint32, C.c_uint32, P32]
+    L.sparsep_partition_by_nnz.argtypes = [P32, C.c_uint32, C.c_uint32, P32]
+    L.sparsep_partition_by_elem.argtypes = [C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]
+    L.sparsep_partition_block_rows.argtypes = [P32, C.c_uint32, P32, C.c_uint32, P32]
+    for s, dt in DTYPES.items():
+        st = STRUCTS[s]
+        PT = C.POINTER(dt.ct)
+        for k in KINDS:
+            f = getattr(L, f"sparsep_plan_{k}_{s}")
+            f.argtypes = [C.POINTER(st[k]), C.POINTER(Opts), C.POINTER(C.c_void_p)]
+            g = getattr(L, f"sparsep_spmv_{k}_{s}")
+            g.argtypes = [C.POINTER(st[k]), PT, PT, C.POINTER(Opts)]
+            h = getattr(L, f"sparsep_free_{k}_{s}")
+            h.argtypes = [C.POINTER(st[k])]
+            h.restype = None
+        for rd in ("read_coo", "read_coo_nopad"):
+            getattr(L, f"sparsep_{rd}_{s}").argtypes = [C.c_char_p, C.POINTER(C.POINTER(st["coo"]))]
+        getattr(L, f"sparsep_read_cooe_{s}").argtypes = [C.c_char_p, C.POINTER(C.POINTER(st["cooe"]))]
+        getattr(L, f"sparsep_sort_cooe_{s}").argtypes = [C.POINTER(st["cooe"])]
+        for name, (a, b, nx) in CONVERTERS.items():
+            f = getattr(L, f"sparsep_{name}_{s}")
+            f.argtypes = [C.POINTER(st[a])] + [C.c_uint32] * nx + [C.POINTER(C.POINTER(st[b]))]
+    _lib = L
+    return L
+
+
+def default_opts(**kw) -> Opts:
+    o = Opts()
+    lib().sparsep_opts_default(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, int(v))
+    return o
+
+
+def ptr(a: np.ndarray | None, ctype) -> Any:
+    if a is None:
+        return C.POINTER(ctype)()
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class HostMatrix:
+    """A reference struct over numpy arrays (the arrays are kept alive here)."""
+
+    def __init__(self, kind: str, dtype: str, struct: C.Structure, arrays: dict[str, np.ndarray],
+                 owned_by_lib: bool = False):
+        self.kind, self.dtype, self.s, self.arrays = kind, dtype, struct, arrays
+        self._owned = owned_by_lib
+
+    @property
+    def ref(self):
+        return C.byref(self.s)
+
+    def __del__(self):
+        if getattr(self, "_owned", False) and _lib is not None:
+            getattr(_lib, f"sparsep_free_{self.kind}_{self.dtype}")(C.pointer(self.s))
+            self._owned = False
+
+
+def _pad(a: np.ndarray, extra: int) -> np.ndarray:
+    out = np.zeros(a.size + extra, dtype=a.dtype)
+    out[: a.size] = a
+    return out
+
+
+def csr(dtype: str, nrows: int, ncols: int, rowptr, colind, values) -> HostMatrix:
+    dt = DTYPES[dtype]
+    rowptr = _pad(np.ascontiguousarray(rowptr, dtype=np.uint32), 1)
+    colind = _pad(np.ascontiguousarray(colind, dtype=np.uint32), 1)
+    values = _pad(np.ascontiguousarray(values, dtype=dt.np), 8)
+    s = STRUCTS[dtype]["csr"](nrows, ncols, int(rowptr[nrows]), ptr(rowptr, C.c_uint32), ptr(colind, C.c_uint32),
+                              ptr(values, dt.ct))
+    return HostMatrix("csr", dtype, s, {"rowptr": rowptr, "colind": colind, "values": values})
+
+
+def elems_array(dtype: str, rows, cols, vals) -> np.ndarray:
+    """numpy structured array with the reference elem_t layout."""
+    E = STRUCTS[dtype]["elem"]
+    n = len(rows)
+    buf = (E * (n + 8))()
+    a = np.ctypeslib.as_array(buf)
+    a["rowind"][:n] = rows
+    a["colind"][:n] = cols
+    a["val"][:n] = vals
+    return a
+
+
+def cooe(dtype: str, nrows: int, ncols: int, rows, cols, vals) -> HostMatrix:
+    el = elems_array(dtype, rows, cols, vals)
+    counts = np.bincount(np.asarray(rows, dtype=np.int64), minlength=nrows).astype(np.uint32)
+    counts = _pad(counts, 1)
+    E = STRUCTS[dtype]["elem"]
+    s = STRUCTS[dtype]["cooe"](nrows, ncols, len(rows), ptr(counts, C.c_uint32), el.ctypes.data_as(C.POINTER(E)))
+    return HostMatrix("cooe", dtype, s, {"rows": counts, "nnzs": el})
+
+
+def coo(dtype: str, nrows: int, ncols: int, rows, cols, vals) -> HostMatrix:
+    dt = DTYPES[dtype]
+    r = _pad(np.ascontiguousarray(rows, dtype=np.uint32), 1)
+    c = _pad(np.ascontiguousarray(cols, dtype=np.uint32), 1)
+    v = _pad(np.ascontiguousarray(vals, dtype=dt.np), 1)
+    s = STRUCTS[dtype]["coo"](nrows, ncols, len(rows), ptr(r, C.c_uint32), ptr(c, C.c_uint32), ptr(v, dt.ct))
+    return HostMatrix("coo", dtype, s, {"rowindx": r, "colind": c, "values": v})
+
+
+def convert(name: str, A: HostMatrix, *args: int) -> HostMatrix:
+    a, b, nx = CONVERTERS[name]
+    assert A.kind == a and len(args) == nx, (A.kind, name, args)
+    out = C.POINTER(STRUCTS[A.dtype][b])()
+    check(getattr(lib(), f"sparsep_{name}_{A.dtype}")(A.ref, *[C.c_uint32(v) for v in args], C.byref(out)), name)
+    return HostMatrix(b, A.dtype, out.contents, {"_src": A}, owned_by_lib=True)
+
+
+def read_mtx(path: str, dtype: str, flavour: str = "coo") -> HostMatrix:
+    kind = "cooe" if flavour == "cooe" else "coo"
+    fn = {"coo": "read_coo", "coo_nopad": "read_coo_nopad", "cooe": "read_cooe"}[flavour]
+    out = C.POINTER(STRUCTS[dtype][kind])()
+    check(getattr(lib(), f"sparsep_{fn}_{dtype}")(str(path).encode(), C.byref(out)), fn)
+    return HostMatrix(kind, dtype, out.contents, {}, owned_by_lib=True)
+
+
+def sort_cooe(A: HostMatrix) -> None:
+    check(getattr(lib(), f"sparsep_sort_cooe_{A.dtype}")(A.ref), "sort_cooe")
+
+
+class Plan:
+    """A device-resident SpMV plan (sparsep_plan)."""
+
+    def __init__(self, A: HostMatrix, opts: Opts | None = None):
+        self.A = A
+        self.dt = DTYPES[A.dtype]
+        h = C.c_void_p()
+        o = opts if opts is not None else default_opts()
+        check(getattr(lib(), f"sparsep_plan_{A.kind}_{A.dtype}")(A.ref, C.byref(o), C.byref(h)),
+              f"plan_{A.kind}_{A.dtype}")
+        self.h = h
+        self.info = PlanInfo()
+        check(lib().sparsep_plan_get_info(self.h, C.byref(self.info)))
+
+    @property
+    def nrows(self) -> int:
+        return int(self.info.nrows)
+
+    @property
+    def ncols(self) -> int:
+        return int(self.info.ncols)
+
+    def run_host(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=self.dt.np)
+        assert x.size >= self.ncols
+        y = np.zeros(self.nrows, dtype=self.dt.np)
+        check(lib().sparsep_execute_host(self.h, x.ctypes.data, y.ctypes.data), "execute_host")
+        return y
+
+    def run_device(self, x_ptr: int, y_ptr: int, stream: int = 0) -> None:
+        check(lib().sparsep_execute_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(stream)),
+              "execute_device")
+
+    def timings(self) -> list[float]:
+        t = (C.c_double * 5)()
+        check(lib().sparsep_timings(self.h, t))
+        return list(t)
+
+    @property
+    def x_ptr(self) -> int:
+        return lib().sparsep_plan_x(self.h)
+
+    @property
+    def y_ptr(self) -> int:
+        return lib().sparsep_plan_y(self.h)
+
+    def free(self) -> None:
+        if getattr(self, "h", None) and self.h.value:
+            lib().sparsep_plan_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def spmv(A: HostMatrix, x: np.ndarray, opts: Opts | None = None) -> np.ndarray:
+    """One-shot SpMV through sparsep_spmv_<kind>_<dtype> (host buffers)."""
+    dt = DTYPES[A.dtype]
+    x = np.ascontiguousarray(x, dtype=dt.np)
+    nrows = A.s.nrows
+    y = np.zeros(nrows, dtype=dt.np)
+    o = opts if opts is not None else default_opts()
+    check(getattr(lib(), f"sparsep_spmv_{A.kind}_{A.dtype}")(A.ref, ptr(x, dt.ct), ptr(y, dt.ct), C.byref(o)),
+          f"spmv_{A.kind}_{A.dtype}")
+    return y

@@ -1,0 +1,19 @@
+// kernels.hpp -- host-side declarations of the kernel launchers (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace sparsep {
+
+// Launch the work-item kernel for format `fmt` (sparsep_format) with one CTA
+// per item.  carry_w = carry slots per item (1 for CSR/COO, rb for BCOO).
+template <typename T>
+cudaError_t launch_items(const Params<T> &P, int fmt, uint32_t carry_w, int threads, size_t smem,
+                         cudaStream_t st);
+
+// y[r] = sum over the V partial slices of row r, in slice order.
+template <typename T>
+cudaError_t launch_merge(const T *part, T *y, uint32_t nrows, uint32_t V, int sms, cudaStream_t st);
+
+}  // namespace sparsep

@@ -1,0 +1,141 @@
+"""Seeded synthetic matrices with the shapes of the benchmark workloads.
+
+The SuiteSparse inputs the reference scripts download are not available, so
+every workload is generated here from a numpy PCG64 stream seeded as stated.
+Matrices are returned as (nrows, ncols, rows, cols, vals) triplets sorted by
+(row, col), plus CSR / BCSR builders.
+
+Workloads (sizes as named):
+  uniform8   4096 x 4096, 8 distinct uniform columns per row, integer values
+             and x in [-8, 8], seed 0 (the plain CSR INT32 correctness case)
+  zipf       1,048,576^2, row lengths Zipf(2.0) capped at 50,000 and rescaled
+             to 16 * 2^20 nonzeros (mean 16), uniform distinct columns,
+             values and x U[-1, 1], seed 1
+  banded     2,097,152 rows, block-banded: block half-bandwidth 32 blocks, 30%
+             of in-band blocks present, 60% fill inside present blocks,
+             integer values U{-4..4} (FP: U[-1, 1]), seed 2
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _dedupe_cols(rng, row_of, ncols, cols):
+    """Redraw duplicate (row, col) pairs until every row has distinct columns."""
+    for _ in range(64):
+        key = row_of.astype(np.int64) * ncols + cols
+        order = np.argsort(key, kind="stable")
+        k = key[order]
+        dup = np.zeros(k.size, dtype=bool)
+        dup[1:] = k[1:] == k[:-1]
+        if not dup.any():
+            return row_of[order], cols[order]
+        bad = order[dup]
+        cols[bad] = rng.integers(0, ncols, bad.size)
+    raise RuntimeError("could not draw distinct columns")
+
+
+def values(rng, n, dtype, lo_int=-8, hi_int=8):
+    dt = np.dtype(dtype)
+    if dt.kind == "f":
+        return rng.uniform(-1.0, 1.0, n).astype(dt)
+    return rng.integers(lo_int, hi_int + 1, n).astype(dt)
+
+
+def uniform_rows(nrows, ncols, per_row, seed, dtype):
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(nrows, dtype=np.uint32), per_row)
+    cols = rng.integers(0, ncols, rows.size).astype(np.int64)
+    rows, cols = _dedupe_cols(rng, rows, ncols, cols)
+    vals = values(rng, rows.size, dtype)
+    x = values(rng, ncols, dtype)
+    return nrows, ncols, rows.astype(np.uint32), cols.astype(np.uint32), vals, x
+
+
+def zipf_lengths(rng, nrows, nnz, a=2.0, cap=50_000):
+    lens = np.minimum(rng.zipf(a, nrows), cap).astype(np.float64)
+    lens = np.maximum(1, np.floor(lens * (nnz / lens.sum()))).astype(np.int64)
+    lens = np.minimum(lens, cap)
+    for _ in range(1000):
+        diff = int(nnz - lens.sum())
+        if diff == 0:
+            break
+        if diff > 0:
+            room = np.nonzero(lens < cap)[0]
+            idx = rng.choice(room, size=min(diff, room.size), replace=False)
+            lens[idx] += 1
+        else:
+            room = np.nonzero(lens > 1)[0]
+            idx = rng.choice(room, size=min(-diff, room.size), replace=False)
+            lens[idx] -= 1
+    assert lens.sum() == nnz
+    return lens
+
+
+def zipf_rows(nrows=1 << 20, ncols=1 << 20, nnz=16 << 20, seed=1, dtype=np.float32, a=2.0, cap=50_000):
+    rng = np.random.default_rng(seed)
+    lens = zipf_lengths(rng, nrows, nnz, a, cap)
+    rows = np.repeat(np.arange(nrows, dtype=np.uint32), lens)
+    cols = rng.integers(0, ncols, rows.size).astype(np.int64)
+    rows, cols = _dedupe_cols(rng, rows, ncols, cols)
+    vals = values(rng, rows.size, dtype)
+    x = values(rng, ncols, dtype)
+    return nrows, ncols, rows.astype(np.uint32), cols.astype(np.uint32), vals, x
+
+
+def to_csr(nrows, rows, cols, vals):
+    """Triplets sorted by (row, col) -> rowptr, colind, values."""
+    rowptr = np.zeros(nrows + 1, dtype=np.uint32)
+    np.cumsum(np.bincount(rows.astype(np.int64), minlength=nrows), out=rowptr[1:])
+    return rowptr, cols.astype(np.uint32), vals
+
+
+def block_banded(nrows=2_097_152, rb=4, cb=4, half_bw=32, p_block=0.3, p_fill=0.6, seed=2, dtype=np.int8):
+    """Block-banded matrix built directly as BCSR arrays.
+
+    Returns dict with nrows, ncols, browptr, bcolind, bval (nblocks x rb x cb,
+    zeros at unfilled positions), nnz (filled positions), nnz_per_block
+    (nonzero values, as the reference's countNNZperBlockBCSRMatrix) and x.
+    """
+    rng = np.random.default_rng(seed)
+    ncols = nrows
+    nbr = (nrows + rb - 1) // rb
+    nbc = (ncols + cb - 1) // cb
+    width = 2 * half_bw + 1
+    present = rng.random((nbr, width)) < p_block
+    jj = np.arange(nbr)[:, None] - half_bw + np.arange(width)[None, :]
+    present &= (jj >= 0) & (jj < nbc)
+    counts = present.sum(axis=1)
+    browptr = np.zeros(nbr + 1, dtype=np.uint32)
+    np.cumsum(counts, out=browptr[1:])
+    bcolind = jj[present].astype(np.uint32)  # row-major -> sorted by column within a block row
+    nb = bcolind.size
+    fill = rng.random((nb, rb, cb)) < p_fill
+    # rows / cols past the matrix edge stay empty
+    brow_of = np.repeat(np.arange(nbr), counts)
+    r_ok = (brow_of[:, None] * rb + np.arange(rb)[None, :]) < nrows
+    c_ok = (bcolind[:, None].astype(np.int64) * cb + np.arange(cb)[None, :]) < ncols
+    fill &= r_ok[:, :, None] & c_ok[:, None, :]
+    dt = np.dtype(dtype)
+    if dt.kind == "f":
+        v = rng.uniform(-1.0, 1.0, (nb, rb, cb)).astype(dt)
+    else:
+        v = rng.integers(-4, 5, (nb, rb, cb)).astype(dt)
+    bval = np.where(fill, v, dt.type(0)).astype(dt)
+    nnz = int(fill.sum())
+    nnz_per_block = (bval != 0).reshape(nb, -1).sum(axis=1).astype(np.uint32)
+    x = rng.uniform(-1.0, 1.0, ncols).astype(dt) if dt.kind == "f" else rng.integers(-4, 5, ncols).astype(dt)
+    return dict(nrows=nrows, ncols=ncols, rb=rb, cb=cb, nbr=nbr, nbc=nbc, browptr=browptr, bcolind=bcolind,
+                bval=bval, nnz=nnz, nnz_per_block=nnz_per_block, x=x, fill=fill)
+
+
+def bcsr_triplets(B):
+    """(rows, cols, vals) of the stored block entries (explicit zeros included)."""
+    rb, cb = B["rb"], B["cb"]
+    nb = B["bcolind"].size
+    counts = np.diff(B["browptr"].astype(np.int64))
+    brow = np.repeat(np.arange(B["nbr"]), counts)
+    r = (brow[:, None, None] * rb + np.arange(rb)[None, :, None]) + 0 * np.arange(cb)[None, None, :]
+    c = (B["bcolind"][:, None, None].astype(np.int64) * cb + np.arange(cb)[None, None, :]) + 0 * np.arange(rb)[None, :, None]
+    m = (r < B["nrows"]) & (c < B["ncols"])
+    return r[m].astype(np.uint32), c[m].astype(np.uint32), B["bval"][m]

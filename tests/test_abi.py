@@ -1,0 +1,98 @@
+"""C-ABI surface (no GPU needed): the library loads and exports every
+function include/sparsep.h declares; host-side error handling returns status
+codes instead of aborting."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import sparsep_b200 as sp
+from sparsep_b200 import capi
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    out = subprocess.run(["gcc", "-E", "-P", "-x", "c", str(ROOT / "include" / "sparsep.h")], capture_output=True,
+                         text=True, check=True).stdout
+    names = set(re.findall(r"\b(sparsep_\w+)\s*\(", out))
+    return sorted(names)
+
+
+def test_exports_every_declared_symbol():
+    L = capi.lib()
+    names = declared_functions()
+    assert len(names) > 300, len(names)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing[:10]
+
+
+def test_version_and_strerror():
+    L = capi.lib()
+    assert b"sm_100a" in L.sparsep_version()
+    for st in (0, -5, -12, -19, -22, -38, -34, -110, -9):
+        assert L.sparsep_strerror(st)
+
+
+def test_options_validation_without_gpu():
+    # invalid options are rejected before any device call
+    A = sp.csr("f32", 2, 2, np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, 2.0], np.float32))
+    h = C.c_void_p()
+    for bad in (dict(lanes=3), dict(lanes=64), dict(nr_workers=17), dict(sync=9), dict(part_balance=7)):
+        o = sp.default_opts(**bad)
+        st = capi.lib().sparsep_plan_csr_f32(A.ref, C.byref(o), C.byref(h))
+        assert st == capi.EINVAL, (bad, st)
+    assert capi.lib().sparsep_plan_csr_f32(None, None, C.byref(h)) in (capi.EINVAL, capi.ENODEV)
+
+
+@pytest.mark.parametrize("content", [
+    "",                                   # empty file
+    "% only a comment\n",                # no header
+    "3 3 2\n1 1 5\n",                     # fewer entries than declared
+    "3 3 1\n1 1 5\n2 2 5\n",              # more entries than declared
+    "3 3 1\n0 1 5\n",                     # 0-based index
+    "3 3 1\n4 1 5\n",                     # row out of range
+    "3 3 1\n1\n",                         # truncated entry
+])
+def test_malformed_mtx(tmp_path, content):
+    p = tmp_path / "bad.mtx"
+    p.write_text(content)
+    for flavour in ("coo", "cooe", "coo_nopad"):
+        with pytest.raises(sp.SparsepError) as e:
+            sp.read_mtx(p, "f32", flavour)
+        assert e.value.status == capi.EBADF
+
+
+def test_missing_file():
+    with pytest.raises(sp.SparsepError) as e:
+        sp.read_mtx("/nonexistent/x.mtx", "i32")
+    assert e.value.status == capi.EBADF
+
+
+def test_converter_validation():
+    # unsorted AoS input is rejected by the 2D converters (they assume sortCOOMatrix ran)
+    A = sp.cooe("f32", 4, 4, np.array([2, 1]), np.array([0, 0]), np.array([1, 1], np.float32))
+    with pytest.raises(sp.SparsepError):
+        sp.convert("cooe2dcsr", A, 2, 2)
+    # zero block size
+    B = sp.csr("f32", 2, 2, np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, 2.0], np.float32))
+    with pytest.raises(sp.SparsepError):
+        sp.convert("csr2bcsr", B, 0, 4)
+    # column index out of range
+    Cx = sp.coo("f32", 2, 2, np.array([0]), np.array([5]), np.array([1.0], np.float32))
+    with pytest.raises(sp.SparsepError):
+        sp.convert("coo2csr", Cx)
+
+
+def test_partition_entry_points():
+    L = capi.lib()
+    s = (C.c_uint32 * 5)()
+    assert L.sparsep_partition_by_row(10, 4, s) == 0
+    assert list(s) == [0, 3, 6, 8, 10]
+    e = (C.c_uint64 * 4)()
+    assert L.sparsep_partition_by_elem(10, 3, e) == 0
+    assert list(e) == [0, 4, 7, 10]
+    assert L.sparsep_partition_by_row(10, 0, s) == capi.EINVAL
