@@ -49,6 +49,10 @@ extern "C" {
 
 const char *sparsep_strerror(int status);
 
+/* Text of the last CUDA runtime error the calling thread's library calls saw
+ * ("" if none); SPARSEP_EIO results carry their cause here. */
+const char *sparsep_last_error(void);
+
 /* ------------------------------------------------------------------------ */
 /* Element types (reference: -DINT8/INT16/INT32/INT64/FP32/FP64)             */
 /* ------------------------------------------------------------------------ */

@@ -49,37 +49,43 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> Path:
+    """checked=True builds libsparsep_b200_check.so with -DSPARSEP_CHECK: every
+    kernel access is bounds-checked and a failed check is reported as a
+    status code instead of touching memory (for diagnosing kernels)."""
+    lib_path = LIB.with_name("libsparsep_b200_check.so") if checked else LIB
+    bdir = BUILD / ("check" if checked else "release")
+    bdir.mkdir(parents=True, exist_ok=True)
     deps = _sources()
-    if not force and not _stale(LIB, deps):
-        return LIB
+    if not force and not _stale(lib_path, deps):
+        return lib_path
+    flags = NVCC_FLAGS + (["-DSPARSEP_CHECK"] if checked else [])
     jobs = []
     objs = []
     for tag, ctype in KERNEL_TYPES.items():
-        o = BUILD / f"kernels_{tag}.o"
+        o = bdir / f"kernels_{tag}.o"
         objs.append(o)
-        jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / "kernels.cu"),
+        jobs.append([nvcc(), *ARCH, *flags, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / "kernels.cu"),
                      "-o", str(o)])
     for src in sorted(CSRC.glob("*.cu")):
         if src.name == "kernels.cu":
             continue
-        o = BUILD / (src.stem + ".o")
+        o = bdir / (src.stem + ".o")
         objs.append(o)
-        jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(o)])
+        jobs.append([nvcc(), *ARCH, *flags, "-c", str(src), "-o", str(o)])
     for src in sorted(CSRC.glob("*.cpp")):
-        o = BUILD / (src.stem + ".o")
+        o = bdir / (src.stem + ".o")
         objs.append(o)
-        jobs.append([nvcc(), *ARCH, *NVCC_FLAGS, "-x", "cu", "-c", str(src), "-o", str(o)])
+        jobs.append([nvcc(), *ARCH, *flags, "-x", "cu", "-c", str(src), "-o", str(o)])
     with cf.ThreadPoolExecutor(max_workers=max(2, os.cpu_count() or 2)) as ex:
         list(ex.map(_run, jobs))
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib_path.with_suffix(".so.tmp")
     _run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
-    os.replace(tmp, LIB)
+    os.replace(tmp, lib_path)
     if verbose:
-        print(f"built {LIB}")
-    return LIB
+        print(f"built {lib_path}")
+    return lib_path
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv)

@@ -9,6 +9,7 @@ module raises if the library is missing.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 from pathlib import Path
 from typing import Any
@@ -16,7 +17,8 @@ from typing import Any
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libsparsep_b200.so"
+# SPARSEP_CHECKED=1 selects the bounds-checked build (libsparsep_b200_check.so)
+LIB_PATH = PKG / ("libsparsep_b200_check.so" if os.environ.get("SPARSEP_CHECKED") == "1" else "libsparsep_b200.so")
 
 # status codes
 OK, EIO, ENOMEM, ENODEV, EINVAL, ENOSYS, ERANGE, ETIMEDOUT, EBADF = 0, -5, -12, -19, -22, -38, -34, -110, -9
@@ -149,6 +151,8 @@ class SparsepError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
         msg = lib().sparsep_strerror(status).decode() if _lib is not None else str(status)
+        if status == EIO and _lib is not None:
+            msg += ": " + _lib.sparsep_last_error().decode()
         super().__init__(f"{what}: {msg} ({status})" if what else f"{msg} ({status})")
 
 
@@ -168,6 +172,7 @@ def lib() -> C.CDLL:
     L = C.CDLL(str(LIB_PATH))
     L.sparsep_strerror.restype = C.c_char_p
     L.sparsep_version.restype = C.c_char_p
+    L.sparsep_last_error.restype = C.c_char_p
     L.sparsep_opts_default.argtypes = [C.POINTER(Opts)]
     L.sparsep_plan_free.argtypes = [C.c_void_p]
     L.sparsep_plan_get_info.argtypes = [C.c_void_p, C.POINTER(PlanInfo)]

@@ -169,8 +169,24 @@ template <typename T> struct Params {
   unsigned long long *carry_val;
   unsigned long long *carry_idx;  // output index or ~0ull
   unsigned int *done;             // completion counter, reset by the last CTA
-  int *err;                       // device error word (bounded waits)
+  int *err;                       // device error word (bounded waits, checked builds)
+  // array extents, used by the bounds-checked build (-DSPARSEP_CHECK)
+  uint64_t n_rowptr, n_idx, n_val, n_elems, n_x, n_xalloc, n_carry;
+  uint32_t nslots, smem_bytes;
 };
+
+// Bounds checks of the checked build: a failed check records `code` in the
+// error word (first failure wins) and the caller skips the access.  The
+// release build compiles them away.
+__device__ __forceinline__ bool sp_flag(int *err, int code) {
+  if (err) atomicCAS(err, 0, code);
+  return true;
+}
+#ifdef SPARSEP_CHECK
+#define SP_BAD(P, cond, code) (!(cond) && ::sparsep::sp_flag((P).err, (code)))
+#else
+#define SP_BAD(P, cond, code) false
+#endif
 
 template <typename T> __device__ __forceinline__ T *out_base(const Params<T> &P, const Item &it) {
   return P.out_mode == OUT_PARTIAL ? P.part + (size_t)it.slot * P.nrows : P.y;
@@ -188,11 +204,20 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 template <typename T>
 __device__ const T *stage_x(const T *x, uint32_t lo, uint32_t w, unsigned char *smem, uint64_t *mbar,
-                            uint32_t &phase, int *err) {
+                            uint32_t &phase, int *err, uint32_t smem_cap, uintptr_t x_end) {
+  (void)smem_cap;
+  (void)x_end;
   uintptr_t gb = reinterpret_cast<uintptr_t>(x) + (uintptr_t)lo * sizeof(T);
   uintptr_t g0 = gb & ~(uintptr_t)15;
   uintptr_t g1 = (gb + (uintptr_t)w * sizeof(T) + 15) & ~(uintptr_t)15;
   uint32_t bytes = (uint32_t)(g1 - g0);
+#ifdef SPARSEP_CHECK
+  if (bytes > smem_cap || g1 > x_end) {
+    if (threadIdx.x == 0 && err) atomicCAS(err, 0, -1017);
+    phase ^= 1u;
+    return x;
+  }
+#endif
   if (threadIdx.x == 0) {
     // order earlier generic-proxy reads of this buffer before the async writes
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

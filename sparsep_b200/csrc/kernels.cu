@@ -35,8 +35,23 @@ __device__ __forceinline__ uint64_t out_index(const Params<T> &P, const Item &it
   return P.out_mode == OUT_PARTIAL ? (uint64_t)it.slot * P.nrows + row : row;
 }
 
+// x element: the staged segment lives in shared memory and must be read with
+// generic loads; the non-coherent read-only path (ld.global.nc) is for x in
+// global memory only.
+template <typename T>
+__device__ __forceinline__ T xload(const T *__restrict__ xb, uint64_t i, bool staged) {
+  return staged ? xb[i] : __ldg(xb + i);
+}
+
+// checked build: x index valid for the staged segment or the whole vector
+template <typename T>
+__device__ __forceinline__ bool x_ok(const Params<T> &P, const Item &it, uint64_t col) {
+  return it.xw > 0 ? (col >= it.xlo && col - it.xlo < it.xw) : col < P.n_x;
+}
+
 template <typename T>
 __device__ __forceinline__ void put(const Params<T> &P, T *out, uint64_t r, Acc<T> v) {
+  if (SP_BAD(P, r < P.nrows, -1004)) return;
   if (P.out_mode == OUT_ATOMIC) atomic_add_out<T>(out + r, v);
   else out[r] = from_acc<T>(v);
 }
@@ -55,18 +70,22 @@ __device__ void csr_rows(const Params<T> &P, const Item &it, const T *__restrict
   const uint64_t r0 = it.a0, r1 = it.a1;
   const uint32_t xoff = it.col_off;
 
-  auto do_row = [&](uint64_t r, bool valid) {
+  auto do_row = [&](uint64_t r, bool valid_in) {
+    bool valid = valid_in;
     A acc = A(0);
+    if (valid && SP_BAD(P, it.ptr_base + r + 1 < P.n_rowptr, -1001)) valid = false;
     if (valid) {
       const uint64_t s = (uint64_t)rp[r] + it.nnz_base, e = (uint64_t)rp[r + 1] + it.nnz_base;
 #pragma unroll 2
       for (uint64_t j = (s & ~3ull) + 4 * gl; j < e; j += 4 * L) {
+        if (SP_BAD(P, j + 3 < P.n_idx && j + 3 < P.n_val, -1002)) break;
         const uint4 c4 = ld_stream4(P.colind + j);
         const Vec4<T> v4 = ld_vals4<T>(P.val + j);
         const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-          if (j + k >= s && j + k < e) acc += mul<T>(v4.v[k], ldx(xb + xoff + cc[k]));
+          if (j + k >= s && j + k < e && !SP_BAD(P, x_ok(P, it, (uint64_t)xoff + cc[k]), -1003))
+            acc += mul<T>(v4.v[k], xload(xb, (uint64_t)xoff + cc[k], it.xw > 0));
       }
     }
 #pragma unroll
@@ -116,12 +135,14 @@ __device__ void csr_long(const Params<T> &P, const Item &it, const T *__restrict
   A acc = A(0);
 #pragma unroll 2
   for (uint64_t j = (s & ~3ull) + 4 * threadIdx.x; j < e; j += 4 * blockDim.x) {
+    if (SP_BAD(P, j + 3 < P.n_idx && j + 3 < P.n_val, -1005)) break;
     const uint4 c4 = ld_stream4(P.colind + j);
     const Vec4<T> v4 = ld_vals4<T>(P.val + j);
     const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (j + k >= s && j + k < e) acc += mul<T>(v4.v[k], ldx(xb + it.col_off + cc[k]));
+      if (j + k >= s && j + k < e && !SP_BAD(P, x_ok(P, it, (uint64_t)it.col_off + cc[k]), -1006))
+        acc += mul<T>(v4.v[k], xload(xb, (uint64_t)it.col_off + cc[k], it.xw > 0));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -131,6 +152,7 @@ __device__ void csr_long(const Params<T> &P, const Item &it, const T *__restrict
     A tot = A(0);
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
     T *out = out_base(P, it);
+    if (SP_BAD(P, it.crow < P.nrows && (P.out_mode == OUT_ATOMIC || item_id < P.n_carry), -1007)) return;
     if (P.out_mode == OUT_ATOMIC) {
       atomic_add_out<T>(out + it.crow, tot);
     } else if (it.chunk == 0) {
@@ -159,6 +181,13 @@ struct Unit {
 template <typename T>
 __device__ __forceinline__ void load_coo4(const Params<T> &P, const Item &it, const T *__restrict__ xb,
                                           uint64_t g, Unit<T, 1> (&u)[4], uint64_t lo, uint64_t hi) {
+  if (SP_BAD(P, 4 * g + 3 < P.n_elems, -1008)) {
+    for (int k = 0; k < 4; ++k) {
+      u[k].key = LLONG_MAX;
+      u[k].v[0] = Acc<T>(0);
+    }
+    return;
+  }
   if constexpr (sizeof(T) <= 4) {
     const char *base = reinterpret_cast<const char *>(P.elems) + g * 48;
     uint4 w0 = ld_stream4(base), w1 = ld_stream4(base + 16), w2 = ld_stream4(base + 32);
@@ -166,13 +195,13 @@ __device__ __forceinline__ void load_coo4(const Params<T> &P, const Item &it, co
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       uint64_t e = 4 * g + k;
-      bool ok = e >= lo && e < hi;
+      bool ok = e >= lo && e < hi && !SP_BAD(P, !(e >= lo && e < hi) || x_ok(P, it, (uint64_t)it.col_off + w[3 * k + 1]), -1009);
       T val;
       if constexpr (sizeof(T) == 1) val = (T)(int8_t)(w[3 * k + 2] & 0xFF);
       else if constexpr (sizeof(T) == 2) val = (T)(int16_t)(w[3 * k + 2] & 0xFFFF);
       else val = __builtin_bit_cast(T, w[3 * k + 2]);
       u[k].key = ok ? (long long)it.row_off + w[3 * k] : LLONG_MAX;
-      u[k].v[0] = ok ? mul<T>(val, ldx(xb + it.col_off + w[3 * k + 1])) : Acc<T>(0);
+      u[k].v[0] = ok ? mul<T>(val, xload(xb, (uint64_t)it.col_off + w[3 * k + 1], it.xw > 0)) : Acc<T>(0);
     }
   } else {
     const char *base = reinterpret_cast<const char *>(P.elems) + g * 64;
@@ -180,10 +209,10 @@ __device__ __forceinline__ void load_coo4(const Params<T> &P, const Item &it, co
     for (int k = 0; k < 4; ++k) {
       uint4 w = ld_stream4(base + 16 * k);
       uint64_t e = 4 * g + k;
-      bool ok = e >= lo && e < hi;
+      bool ok = e >= lo && e < hi && !SP_BAD(P, !(e >= lo && e < hi) || x_ok(P, it, (uint64_t)it.col_off + w.y), -1009);
       T val = __builtin_bit_cast(T, ((unsigned long long)w.w << 32) | w.z);
       u[k].key = ok ? (long long)it.row_off + w.x : LLONG_MAX;
-      u[k].v[0] = ok ? mul<T>(val, ldx(xb + it.col_off + w.y)) : Acc<T>(0);
+      u[k].v[0] = ok ? mul<T>(val, xload(xb, (uint64_t)it.col_off + w.y, it.xw > 0)) : Acc<T>(0);
     }
   }
 }
@@ -220,12 +249,14 @@ __device__ __forceinline__ void load_brow(const T *p, T (&v)[CB]) {
 // RB = CB = 0 selects the runtime-size path (rb <= 16).
 template <typename T, int RB, int CB>
 __device__ __forceinline__ void block_mv(const Params<T> &P, const T *__restrict__ xb, uint64_t b, uint32_t J,
-                                         uint32_t col_off, Acc<T> *acc) {
+                                         uint32_t col_off, Acc<T> *acc, const Item &it) {
+  if (SP_BAD(P, (b + 1) * P.rb * P.cb <= P.n_val, -1010)) return;
   if constexpr (RB > 0) {
     const uint64_t c0 = (uint64_t)col_off + (uint64_t)J * CB;
     T xv[CB];
 #pragma unroll
-    for (int c = 0; c < CB; ++c) xv[c] = (c0 + c < P.ncols) ? ldx(xb + c0 + c) : T(0);
+    for (int c = 0; c < CB; ++c)
+      xv[c] = (c0 + c < P.ncols && !SP_BAD(P, x_ok(P, it, c0 + c), -1011)) ? xload(xb, c0 + c, it.xw > 0) : T(0);
     const T *bp = P.bval + b * (RB * CB);
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
@@ -240,7 +271,8 @@ __device__ __forceinline__ void block_mv(const Params<T> &P, const T *__restrict
     const T *bp = P.bval + b * rb * cb;
     for (uint32_t c = 0; c < cb; ++c) {
       if (c0 + c >= P.ncols) break;
-      T xv = ldx(xb + c0 + c);
+      if (SP_BAD(P, x_ok(P, it, c0 + c), -1011)) break;
+      T xv = xload(xb, c0 + c, it.xw > 0);
       for (uint32_t r = 0; r < rb; ++r) acc[r] += mul<T>(bp[r * cb + c], xv);
     }
   }
@@ -267,9 +299,12 @@ __device__ void bcsr_rows(const Params<T> &P, const Item &it, const T *__restric
     A acc[RMAX];
 #pragma unroll
     for (int r = 0; r < RMAX; ++r) acc[r] = A(0);
-    if (valid) {
+    if (valid && !SP_BAD(P, it.ptr_base + br + 1 < P.n_rowptr, -1012)) {
       const uint64_t s = (uint64_t)bp[br] + it.nnz_base, e = (uint64_t)bp[br + 1] + it.nnz_base;
-      for (uint64_t b = s + gl; b < e; b += L) block_mv<T, RB, CB>(P, xb, b, __ldcs(P.bcolind + b), it.col_off, acc);
+      for (uint64_t b = s + gl; b < e; b += L) {
+        if (SP_BAD(P, b < P.n_idx, -1013)) break;
+        block_mv<T, RB, CB>(P, xb, b, __ldcs(P.bcolind + b), it.col_off, acc, it);
+      }
     }
 #pragma unroll
     for (int r = 0; r < RMAX; ++r) {
@@ -309,7 +344,7 @@ __device__ __forceinline__ void zero_rows(const Params<T> &P, const Item &it, T 
   for (long long k = k0 + 1; k < k1; ++k)
     for (uint32_t r = 0; r < (W == 1 ? 1u : rb); ++r) {
       const uint64_t row = key_row<T, W>(it, k, r, rb);
-      if (row < it.row_end) out[row] = T(0);
+      if (row < it.row_end && !SP_BAD(P, row < P.nrows, -1015)) out[row] = T(0);
     }
 }
 
@@ -321,6 +356,7 @@ __device__ __forceinline__ void write_run(const Params<T> &P, const Item &it, T 
     if (r >= (int)rb) break;
     const uint64_t row = key_row<T, W>(it, key, r, rb);
     if (row >= it.row_end) continue;
+    if (SP_BAD(P, row < P.nrows, -1015)) continue;
     if (atomic) atomic_add_out<T>(out + row, v[r]);
     else out[row] = from_acc<T>(v[r]);
   }
@@ -339,10 +375,10 @@ __device__ __forceinline__ void load_units(const Params<T> &P, const Item &it, c
 #pragma unroll
     for (int r = 0; r < W; ++r) u[0].v[r] = Acc<T>(0);
     u[0].key = LLONG_MAX;
-    if (ok) {
+    if (ok && !SP_BAD(P, b < P.n_elems, -1014)) {
       const sparsep_bind bi = P.bind[b];
       u[0].key = (long long)bi.rowind;
-      block_mv<T, RB, CB>(P, xb, b, bi.colind, it.col_off, u[0].v);
+      block_mv<T, RB, CB>(P, xb, b, bi.colind, it.col_off, u[0].v, it);
     }
   }
 }
@@ -356,11 +392,13 @@ __device__ void elems_lf(const Params<T> &P, const Item &it, const T *__restrict
   constexpr int K = (W == 1) ? COO_K : 1;
   __shared__ KVT scan_smem[32];
   __shared__ KVT tail_smem;
+  __shared__ long long heads_smem[512];
   T *out = out_base(P, it);
   const uint32_t rb = W == 1 ? 1u : (RB > 0 ? RB : P.rb);
   const uint64_t lo = it.a0, hi = it.a1;
   const bool atomic = P.out_mode == OUT_ATOMIC;
 
+  if (SP_BAD(P, (uint64_t)(item_id + 1) * cw <= P.n_carry || atomic, -1018)) return;
   if (lo >= hi) {  // empty: only zero the owned rows
     if (!atomic && threadIdx.x == 0) zero_rows<T, W>(P, it, out, (long long)it.own0 - 1, it.own1, rb);
     if (!atomic && threadIdx.x < cw) P.carry_idx[(uint64_t)item_id * cw + threadIdx.x] = NO_CARRY;
@@ -419,8 +457,16 @@ __device__ void elems_lf(const Params<T> &P, const Item &it, const T *__restrict
     mine.k = tail;
 #pragma unroll
     for (int i = 0; i < W; ++i) mine.v[i] = run[i];
+    heads_smem[threadIdx.x] = any ? head : LLONG_MAX;  // read after the scan's barriers
     KVT ex, in;
     block_seg_scan<A, W>(mine, carry, ex, in, scan_smem);
+    const uint64_t last_g = (g_last < cg + blockDim.x ? g_last : cg + blockDim.x) - 1;
+    // a tail run is complete when the next thread starts another key; the
+    // chunk's last thread hands its tail on instead
+    if (any && g != last_g && heads_smem[threadIdx.x + 1] != tail) write_run<T, W>(P, it, out, tail, in.v, rb, atomic);
+    // likewise the run handed over by the previous chunk
+    if (threadIdx.x == 0 && carry.k >= (long long)it.own0 && head != carry.k)
+      write_run<T, W>(P, it, out, carry.k, carry.v, rb, atomic);
     if (any) {
       if (!atomic) zero_rows<T, W>(P, it, out, ex.k, head, rb);
       if (head != tail) {
@@ -431,7 +477,6 @@ __device__ void elems_lf(const Params<T> &P, const Item &it, const T *__restrict
       }
     }
     // the chunk's last thread with units hands its tail to the next chunk
-    const uint64_t last_g = (g_last < cg + blockDim.x ? g_last : cg + blockDim.x) - 1;
     if (g == last_g) tail_smem = in;
     __syncthreads();
     carry = tail_smem;
@@ -466,6 +511,7 @@ __device__ void carry_fixup(const Params<T> &P, uint32_t nslots, uint32_t W) {
   for (uint32_t s = threadIdx.x; s < nslots; s += blockDim.x) {
     const unsigned long long idx = __ldcg(P.carry_idx + s);
     if (idx == NO_CARRY) continue;
+    if (SP_BAD(P, idx < (uint64_t)P.nslots * P.nrows, -1016)) continue;
     if (s >= W && __ldcg(P.carry_idx + s - W) == idx) continue;  // not the first of its run
     A sum = bits_acc<A>(__ldcg(P.carry_val + s));
     for (uint32_t t = s + W; t < nslots && __ldcg(P.carry_idx + t) == idx; t += W)
@@ -490,7 +536,8 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
   if (it.xw > 0) {
     uint32_t phase = 0;
     mbar_init(&mbar);
-    xb = stage_x<T>(P.x, it.xlo, it.xw, dyn_smem, &mbar, phase, P.err);
+    xb = stage_x<T>(P.x, it.xlo, it.xw, dyn_smem, &mbar, phase, P.err, P.smem_bytes,
+                    reinterpret_cast<uintptr_t>(P.x + P.n_xalloc));
   }
 
   if constexpr (FMT == SPARSEP_FMT_CSR) {
@@ -524,6 +571,7 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
 
   // lock-free carries: the last CTA to finish adds them (threadfence reduction)
   if (P.carry_idx != nullptr && P.out_mode != OUT_ATOMIC) {
+    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();

@@ -47,6 +47,7 @@ struct sparsep_plan {
   unsigned long long *carry_val = nullptr, *carry_idx = nullptr;
   unsigned int *done = nullptr;
   int *err = nullptr;
+  uint64_t n_rowptr = 0, n_idx = 0, n_val = 0, n_elems = 0;  // allocated extents
   bool stage = false;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[5] = {};
@@ -54,7 +55,10 @@ struct sparsep_plan {
   sparsep_plan_info info{};
 };
 
+static thread_local char g_last_error[256] = "";
+
 static int map_cuda(cudaError_t e) {
+  if (e != cudaSuccess) std::snprintf(g_last_error, sizeof g_last_error, "%s (%d)", cudaGetErrorString(e), (int)e);
   switch (e) {
     case cudaSuccess: return SPARSEP_OK;
     case cudaErrorMemoryAllocation: return SPARSEP_ENOMEM;
@@ -394,6 +398,8 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
   if ((st = upload(p, A->rowptr, (size_t)A->nrows + 1, 4, 16, (const void **)&p->rowptr))) return st;
   if ((st = upload(p, A->colind, A->nnz, 4, 16, (const void **)&p->colind))) return st;
   if ((st = upload(p, A->values, A->nnz, sizeof(T), 16, &p->val))) return st;
+  p->n_rowptr = (uint64_t)A->nrows + 17;
+  p->n_idx = p->n_val = (uint64_t)A->nnz + 16;
   p->info.compulsory_bytes = compulsory_csr(A->nnz, A->nrows, A->ncols, sizeof(T));
   if ((st = finish_plan(p, items, oo))) return st;
   p->t[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -431,6 +437,8 @@ static int plan_csr_tiles(int scheme, uint32_t nrows, uint32_t ncols, uint64_t n
   if ((st = upload(p, drowptr, rowptr_len, 4, 16, (const void **)&p->rowptr))) return st;
   if ((st = upload(p, dcolind, nnz, 4, 16, (const void **)&p->colind))) return st;
   if ((st = upload(p, dval, nnz, sizeof(T), 16, &p->val))) return st;
+  p->n_rowptr = rowptr_len + 16;
+  p->n_idx = p->n_val = nnz + 16;
   p->info.compulsory_bytes = compulsory_csr(nnz, nrows, ncols, sizeof(T));
   if ((st = finish_plan(p, items, oo))) return st;
   p->t[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -569,11 +577,14 @@ static int plan_elems(int fmt, int scheme, uint32_t nrows, uint32_t ncols, uint6
   set_out_mode(p, oo, V, true, W);
   if (fmt == SPARSEP_FMT_COO) {
     if ((st = upload(p, elems, nunits, elem_size, 8, &p->elems))) return st;
+    p->n_elems = nunits + 8;
     p->info.compulsory_bytes = nnz * (8 + sizeof(T)) + (uint64_t)ncols * sizeof(T) + (uint64_t)nrows * sizeof(T);
   } else {
     p->nblocks = nunits;
     if ((st = upload(p, B->bind, nunits, sizeof(sparsep_bind), 4, (const void **)&p->bind))) return st;
     if ((st = upload(p, B->bval, nunits * rb * cb, sizeof(T), 16 * rb * cb, &p->bval))) return st;
+    p->n_elems = nunits + 4;
+    p->n_val = (nunits + 16) * rb * cb;
     p->info.compulsory_bytes = nunits * (8 + (uint64_t)rb * cb * sizeof(T)) + (uint64_t)ncols * sizeof(T) +
                                (uint64_t)nrows * sizeof(T);
   }
@@ -841,6 +852,9 @@ static int plan_bcsr_tiles(int scheme, uint32_t nrows, uint32_t ncols, uint64_t 
   if ((st = upload(p, browptr, browptr_len, 4, 16, (const void **)&p->rowptr))) return st;
   if ((st = upload(p, bcolind, nblocks, 4, 16, (const void **)&p->bcolind))) return st;
   if ((st = upload(p, bval, nblocks * rb * cb, sizeof(T), 16 * rb * cb, &p->bval))) return st;
+  p->n_rowptr = browptr_len + 16;
+  p->n_idx = nblocks + 16;
+  p->n_val = (nblocks + 16) * rb * cb;
   uint64_t nbr = (nrows + rb - 1) / rb;
   p->info.compulsory_bytes = nblocks * (4 + (uint64_t)rb * cb * sizeof(T)) + (nbr + 1) * 4 +
                              (uint64_t)ncols * sizeof(T) + (uint64_t)nrows * sizeof(T);
@@ -1160,6 +1174,15 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   P.carry_idx = p->carry_w ? p->carry_idx : nullptr;
   P.done = p->done;
   P.err = p->err;
+  P.n_rowptr = p->n_rowptr;
+  P.n_idx = p->n_idx;
+  P.n_val = p->n_val;
+  P.n_elems = p->n_elems;
+  P.n_x = p->ncols;
+  P.n_xalloc = x == p->xpad ? (uint64_t)p->ncols + 64 : p->ncols;  // staging reads into the slack
+  P.n_carry = p->carry_w ? (uint64_t)p->nitems * p->carry_w + 1 : 0;
+  P.nslots = p->out_mode == OUT_PARTIAL ? p->V : 1;
+  P.smem_bytes = (uint32_t)p->smem;
   CK(launch_items<T>(P, p->format, p->carry_w, p->threads, p->smem, s));
   if (p->out_mode == OUT_PARTIAL) {
     CK(cudaEventRecord(p->ev[2], s));
@@ -1196,7 +1219,15 @@ static int check_err(sparsep_plan *p) {
 // ---------------------------------------------------------------------------
 extern "C" {
 
-const char *sparsep_version(void) { return "sparsep_b200 0.1 (sm_100a)"; }
+const char *sparsep_version(void) {
+#ifdef SPARSEP_CHECK
+  return "sparsep_b200 0.1 (sm_100a, bounds-checked)";
+#else
+  return "sparsep_b200 0.1 (sm_100a)";
+#endif
+}
+
+const char *sparsep_last_error(void) { return g_last_error; }
 
 const char *sparsep_strerror(int s) {
   switch (s) {

@@ -69,11 +69,14 @@ def padded_x(kind: str, A: capi.HostMatrix, x: np.ndarray) -> np.ndarray:
 
 
 def oracle_spmv(A: capi.HostMatrix, x: np.ndarray) -> np.ndarray:
+    if A.kind == "coo":
+        # the reference never multiplies the unsorted SoA COO directly: it
+        # converts it with coo2csr first (spmv/1D/CSR-row/host/app.c:101-103)
+        return oracle_spmv(sp.convert("coo2csr", A), x)
     dt = capi.DTYPES[A.dtype]
     xp = padded_x(A.kind, A, np.ascontiguousarray(x, dtype=dt.np))
     y = np.zeros(ylen_ref(A.kind, A.s) + 8, dtype=dt.np)
-    kind = "cooe" if A.kind == "coo" else A.kind
-    f = getattr(oracle(), f"oracle_spmv_{kind}_{A.dtype}")
+    f = getattr(oracle(), f"oracle_spmv_{A.kind}_{A.dtype}")
     f(y.ctypes.data_as(C.c_void_p), A.ref, xp.ctypes.data_as(C.c_void_p))
     return y[: int(A.s.nrows)]
 
