@@ -125,6 +125,125 @@ __device__ void csr_rows(const Params<T> &P, const Item &it, const T *__restrict
 }
 
 // ---------------------------------------------------------------------------
+// CSR rows, staged ("stream") form used when lanes = auto.  A chunk of up to
+// CSR_RCAP rows / CSR_CAP nonzeros is moved in three coalesced sweeps: its
+// rowptr slice into shared memory, then every nonzero (128-bit loads of colind
+// and values) times its gathered x into a shared product array; rows are then
+// summed from shared memory (a thread per short row, a warp per long row) and
+// written with consecutive threads on consecutive rows.  A row longer than the
+// chunk capacity is reduced by the whole CTA straight from global memory.
+// ---------------------------------------------------------------------------
+constexpr int CSR_CAP = 4096;   // nonzeros per chunk
+constexpr int CSR_RCAP = 1024;  // rows per chunk
+constexpr int CSR_SHORT = 48;   // rows up to this length are summed by one thread
+
+// sum of a[s, e) x over the whole CTA (thread 0 gets the total)
+template <typename T>
+__device__ Acc<T> cta_range_sum(const Params<T> &P, const Item &it, const T *__restrict__ xb, uint64_t s,
+                                uint64_t e, Acc<T> *red) {
+  using A = Acc<T>;
+  A acc = A(0);
+#pragma unroll 2
+  for (uint64_t j = (s & ~3ull) + 4 * threadIdx.x; j < e; j += 4 * blockDim.x) {
+    if (SP_BAD(P, j + 3 < P.n_idx && j + 3 < P.n_val, -1005)) break;
+    const uint4 c4 = ld_stream4(P.colind + j);
+    const Vec4<T> v4 = ld_vals4<T>(P.val + j);
+    const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (j + k >= s && j + k < e && !SP_BAD(P, x_ok(P, it, (uint64_t)it.col_off + cc[k]), -1006))
+        acc += mul<T>(v4.v[k], xload(xb, (uint64_t)it.col_off + cc[k], it.xw > 0));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __syncthreads();  // red may still be read from a previous call
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  A tot = A(0);
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+  return tot;
+}
+
+template <typename T>
+__device__ void csr_stream(const Params<T> &P, const Item &it, const T *__restrict__ xb) {
+  using A = Acc<T>;
+  __shared__ A prods[CSR_CAP];
+  __shared__ uint32_t srp[CSR_RCAP + 1];
+  __shared__ uint32_t longs[CSR_RCAP];
+  __shared__ uint32_t nlong;
+  __shared__ A red[32];
+  T *out = out_base(P, it);
+  const uint32_t *rp = P.rowptr + it.ptr_base;
+  const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool staged = it.xw > 0;
+  uint64_t r = it.a0;
+  while (r < it.a1) {
+    const uint32_t nr = (uint32_t)((it.a1 - r) < CSR_RCAP ? (it.a1 - r) : CSR_RCAP);
+    if (SP_BAD(P, it.ptr_base + r + nr < P.n_rowptr, -1001)) return;
+    for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) srp[i] = __ldcs(rp + r + i);
+    if (threadIdx.x == 0) nlong = 0;
+    __syncthreads();
+    // rows [r, r+k) form the chunk: the longest prefix within CSR_CAP nonzeros
+    const uint32_t base = srp[0];
+    uint32_t k = nr;
+    if (srp[nr] - base > (uint32_t)CSR_CAP) {
+      uint32_t lo = 0, hi = nr;  // largest k with srp[k] - base <= CAP
+      while (lo < hi) {
+        const uint32_t m = (lo + hi + 1) >> 1;
+        if (srp[m] - base <= (uint32_t)CSR_CAP) lo = m; else hi = m - 1;
+      }
+      k = lo;
+    }
+    if (k == 0) {  // one row longer than the chunk: whole-CTA reduction from global
+      const A tot = cta_range_sum<T>(P, it, xb, (uint64_t)base + it.nnz_base, (uint64_t)srp[1] + it.nnz_base, red);
+      if (threadIdx.x == 0) put<T>(P, out, it.row_off + r, tot);
+      __syncthreads();
+      r += 1;
+      continue;
+    }
+    const uint64_t s0 = (uint64_t)base + it.nnz_base, e0 = (uint64_t)srp[k] + it.nnz_base;
+    for (uint64_t g = (s0 >> 2) + threadIdx.x; 4 * g < e0; g += blockDim.x) {
+      const uint64_t j = 4 * g;
+      if (SP_BAD(P, j + 3 < P.n_idx && j + 3 < P.n_val, -1002)) break;
+      const uint4 c4 = ld_stream4(P.colind + j);
+      const Vec4<T> v4 = ld_vals4<T>(P.val + j);
+      const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (j + q >= s0 && j + q < e0) {
+          const uint64_t col = (uint64_t)it.col_off + cc[q];
+          prods[j + q - s0] = SP_BAD(P, x_ok(P, it, col), -1003) ? A(0) : mul<T>(v4.v[q], xload(xb, col, staged));
+        }
+    }
+    __syncthreads();
+    // short rows: one thread each; long rows are queued for the warps
+    for (uint32_t i = threadIdx.x; i < k; i += blockDim.x) {
+      const uint32_t a = srp[i] - base, b = srp[i + 1] - base;
+      if (b - a <= (uint32_t)CSR_SHORT) {
+        A acc = A(0);
+        for (uint32_t q = a; q < b; ++q) acc += prods[q];
+        put<T>(P, out, it.row_off + r + i, acc);
+      } else {
+        longs[atomicAdd(&nlong, 1u)] = i;
+      }
+    }
+    __syncthreads();
+    for (uint32_t li = warp; li < nlong; li += nw) {
+      const uint32_t i = longs[li];
+      const uint32_t a = srp[i] - base, b = srp[i + 1] - base;
+      A acc = A(0);
+      for (uint32_t q = a + lane; q < b; q += 32) acc += prods[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) put<T>(P, out, it.row_off + r + i, acc);
+    }
+    __syncthreads();
+    r += k;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // CSR long-row chunk: all threads reduce elements [a0, a1) of row crow.
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -545,6 +664,7 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
       csr_long<T>(P, it, xb, item_id);
     } else {
       switch (it.lanes) {
+        case 0: csr_stream<T>(P, it, xb); break;
         case 1: csr_rows<T, 1>(P, it, xb); break;
         case 2: csr_rows<T, 2>(P, it, xb); break;
         case 4: csr_rows<T, 4>(P, it, xb); break;
@@ -609,9 +729,12 @@ __global__ void merge_partials(const T *__restrict__ part, T *__restrict__ y, ui
 template <typename T, int FMT, int RB, int CB>
 static cudaError_t launch_t(const Params<T> &P, uint32_t carry_w, int threads, size_t smem, cudaStream_t st) {
   auto k = spmv_items<T, FMT, RB, CB>;
-  if (smem > 48 * 1024) {
+  // the default dynamic limit is 48 KB minus the kernel's static shared memory
+  static int configured = 0;
+  if (smem > 0 && (int)smem > configured) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    configured = (int)smem;
   }
   k<<<P.nitems, threads, smem, st>>>(P, carry_w);
   return cudaGetLastError();

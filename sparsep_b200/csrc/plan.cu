@@ -110,7 +110,7 @@ static uint32_t pow2ceil(uint64_t v) {
 
 // Auto-planner sizes: one CTA of 256 threads takes ~4k nonzeros.
 static constexpr uint64_t AUTO_ITEM_NNZ = 4096;
-static constexpr uint64_t AUTO_ITEM_ROWS = 2048;
+static constexpr uint64_t AUTO_ITEM_ROWS = 1024;
 static constexpr uint64_t AUTO_LONG_CHUNK = 8192;
 static constexpr uint64_t AUTO_ITEM_ELEMS = 4096;
 static constexpr uint64_t AUTO_ITEM_ENTRIES = 8192;  // stored block entries per item
@@ -157,11 +157,6 @@ static Item make_item(const Tile &t, uint16_t kind) {
   return it;
 }
 
-static uint16_t auto_lanes_rows(uint64_t nnz, uint64_t rows) {
-  if (rows == 0) return 1;
-  uint64_t mean = (nnz + rows - 1) / rows;
-  return (uint16_t)pow2ceil((mean + 3) / 4);
-}
 
 // CSR rows [r0, r1) of a tile (local rowptr rp) -> items.  faithful: exactly one
 // item; otherwise split by nnz, with rows longer than AUTO_ITEM_NNZ chunked
@@ -173,7 +168,8 @@ static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32
     Item it = make_item(t, ITEM_ROWS);
     it.a0 = a;
     it.a1 = b;
-    it.lanes = o.lanes ? (uint16_t)o.lanes : auto_lanes_rows((uint64_t)rp[b] - rp[a], b - a);
+    // lanes = 0 selects the staged (stream) row kernel, a fixed L the vector kernel
+    it.lanes = (uint16_t)o.lanes;
     it.worker_bal = o.worker_balance == SPARSEP_BAL_NNZ_ELEM || o.worker_balance == SPARSEP_BAL_BLOCK
                         ? SPARSEP_BAL_NNZ
                         : (uint32_t)o.worker_balance;
@@ -298,12 +294,13 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   p->info.kernel_launches = 1 + (p->out_mode == OUT_PARTIAL ? 1 : 0);
   p->info.workers = workers;
   p->info.stage_x = p->stage ? 1 : 0;
-  int lanes_min = 32, lanes_max = 1;
-  for (const Item &it : items) {
-    lanes_min = std::min<int>(lanes_min, it.lanes ? it.lanes : 1);
-    lanes_max = std::max<int>(lanes_max, it.lanes ? it.lanes : 1);
-  }
-  p->info.lanes = items.empty() ? 0 : (lanes_min == lanes_max ? lanes_min : 0);
+  int lanes_min = 64, lanes_max = -1;  // over row items; 0 = staged stream kernel
+  for (const Item &it : items)
+    if (it.kind == ITEM_ROWS) {
+      lanes_min = std::min<int>(lanes_min, it.lanes);
+      lanes_max = std::max<int>(lanes_max, it.lanes);
+    }
+  p->info.lanes = lanes_max < 0 ? 0 : (lanes_min == lanes_max ? lanes_min : -1);
   static const char *fm[] = {"csr", "coo", "bcsr", "bcoo"};
   static const char *sc[] = {"1d", "2d-d", "2d-rbd", "2d-bd"};
   static const char *sy[] = {"lf", "atomic", "atomic(cg)"};
