@@ -62,13 +62,14 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
     flags = NVCC_FLAGS + (["-DSPARSEP_CHECK"] if checked else [])
     jobs = []
     objs = []
+    per_type = ("kernels.cu", "csr_pipe.cu")
     for tag, ctype in KERNEL_TYPES.items():
-        o = bdir / f"kernels_{tag}.o"
-        objs.append(o)
-        jobs.append([nvcc(), *ARCH, *flags, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / "kernels.cu"),
-                     "-o", str(o)])
+        for name in per_type:
+            o = bdir / f"{Path(name).stem}_{tag}.o"
+            objs.append(o)
+            jobs.append([nvcc(), *ARCH, *flags, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / name), "-o", str(o)])
     for src in sorted(CSRC.glob("*.cu")):
-        if src.name == "kernels.cu":
+        if src.name in per_type:
             continue
         o = bdir / (src.stem + ".o")
         objs.append(o)

@@ -141,6 +141,10 @@ struct Item {
   uint32_t chunk;       // ITEM_LONG: chunk index within the row (0 owns the row)
   uint32_t worker_bal;  // ITEM_ROWS: sparsep_balance across warps
   uint32_t row_end;     // exclusive bound on output rows this item may write
+  uint64_t n0, n1;      // CSR: absolute nonzero range of the item (for bulk prefetch)
+  uint32_t nchunk;      // ITEM_LONG: chunks of the row
+  uint32_t first;       // ITEM_LONG: item index of the row's chunk 0
+  uint32_t cslot;       // ITEM_LONG: the row's arrival counter
 };
 
 // Per-launch parameters shared by all kernels.
@@ -169,6 +173,7 @@ template <typename T> struct Params {
   unsigned long long *carry_val;
   unsigned long long *carry_idx;  // output index or ~0ull
   unsigned int *done;             // completion counter, reset by the last CTA
+  unsigned int *row_cnt;          // per long row arrival counters (pipelined CSR)
   int *err;                       // device error word (bounded waits, checked builds)
   // array extents, used by the bounds-checked build (-DSPARSEP_CHECK)
   uint64_t n_rowptr, n_idx, n_val, n_elems, n_x, n_xalloc, n_carry;

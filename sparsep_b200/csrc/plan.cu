@@ -47,8 +47,11 @@ struct sparsep_plan {
   unsigned long long *carry_val = nullptr, *carry_idx = nullptr;
   unsigned int *done = nullptr;
   int *err = nullptr;
+  unsigned int *row_cnt = nullptr;  // long-row arrival counters (pipelined CSR)
   uint64_t n_rowptr = 0, n_idx = 0, n_val = 0, n_elems = 0;  // allocated extents
   bool stage = false;
+  bool pipe = false;  // 1D CSR auto items run on the pipelined persistent kernel
+  int pipe_grid = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[5] = {};
   double t[5] = {0, 0, 0, 0, 0};
@@ -108,10 +111,12 @@ static uint32_t pow2ceil(uint64_t v) {
   return p;
 }
 
-// Auto-planner sizes: one CTA of 256 threads takes ~4k nonzeros.
-static constexpr uint64_t AUTO_ITEM_NNZ = 4096;
+// Auto-planner sizes: one CTA of 256 threads takes ~4k nonzeros.  Row items
+// hold at most 4096 - 16 nonzeros so that, after the 16-byte alignment of the
+// staged copy, they fit the pipelined kernel's 4096 slots.
+static constexpr uint64_t AUTO_ITEM_NNZ = 4080;
 static constexpr uint64_t AUTO_ITEM_ROWS = 1024;
-static constexpr uint64_t AUTO_LONG_CHUNK = 8192;
+static constexpr uint64_t AUTO_LONG_CHUNK = 4096;
 static constexpr uint64_t AUTO_ITEM_ELEMS = 4096;
 static constexpr uint64_t AUTO_ITEM_ENTRIES = 8192;  // stored block entries per item
 static constexpr size_t STAGE_AUTO_MAX = 96 * 1024;
@@ -168,6 +173,8 @@ static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32
     Item it = make_item(t, ITEM_ROWS);
     it.a0 = a;
     it.a1 = b;
+    it.n0 = t.nnz_base + rp[a];
+    it.n1 = t.nnz_base + rp[b];
     // lanes = 0 selects the staged (stream) row kernel, a fixed L the vector kernel
     it.lanes = (uint16_t)o.lanes;
     it.worker_bal = o.worker_balance == SPARSEP_BAL_NNZ_ELEM || o.worker_balance == SPARSEP_BAL_BLOCK
@@ -185,12 +192,17 @@ static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32
     if (allow_long && len > AUTO_ITEM_NNZ) {
       emit(a, r);
       uint64_t nch = (len + AUTO_LONG_CHUNK - 1) / AUTO_LONG_CHUNK;
+      const uint32_t first = (uint32_t)items.size();
       for (uint64_t c = 0; c < nch; ++c) {
         Item it = make_item(t, ITEM_LONG);
         it.a0 = t.nnz_base + rp[r] + c * AUTO_LONG_CHUNK;
         it.a1 = std::min<uint64_t>(t.nnz_base + rp[r + 1], it.a0 + AUTO_LONG_CHUNK);
         it.crow = (uint32_t)(t.row_off + r);
         it.chunk = (uint32_t)c;
+        it.n0 = it.a0;
+        it.n1 = it.a1;
+        it.nchunk = (uint32_t)nch;
+        it.first = first;  // cslot is numbered by number_long_rows()
         it.lanes = 32;
         items.push_back(it);
       }
@@ -206,6 +218,16 @@ static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32
     acc += len;
   }
   emit(a, r1);
+}
+
+// Long-row arrival counters: one per long row, numbered in item order.
+static void number_long_rows(std::vector<Item> &items) {
+  uint32_t n = 0;
+  for (Item &it : items)
+    if (it.kind == ITEM_LONG) {
+      if (it.chunk == 0) ++n;
+      it.cslot = n - 1;
+    }
 }
 
 // Element (COO) / block (BCOO) range [e0, e1) of a tile whose keys (rows or
@@ -268,6 +290,13 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   }
   st = dalloc(p, 16, (void **)&p->err);
   if (st) return st;
+  uint32_t nlong = 0;
+  for (const Item &it : items) nlong += it.kind == ITEM_LONG && it.chunk == 0;
+  if (nlong) {
+    st = dalloc(p, (size_t)nlong * 4, (void **)&p->row_cnt);
+    if (st) return st;
+    p->info.scratch_bytes += (size_t)nlong * 4;
+  }
   size_t smem = 0;
   for (const Item &it : items) {
     if (it.xw) {
@@ -304,9 +333,9 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   static const char *fm[] = {"csr", "coo", "bcsr", "bcoo"};
   static const char *sc[] = {"1d", "2d-d", "2d-rbd", "2d-bd"};
   static const char *sy[] = {"lf", "atomic", "atomic(cg)"};
-  std::snprintf(p->info.variant, sizeof p->info.variant, "%s/%s/%s/parts=%d/lanes=%s/V=%u%s", fm[p->format],
+  std::snprintf(p->info.variant, sizeof p->info.variant, "%s/%s/%s/parts=%d/lanes=%s/V=%u%s%s", fm[p->format],
                 sc[p->scheme], sy[o.sync], o.nr_parts, o.lanes ? std::to_string(o.lanes).c_str() : "auto", p->V,
-                p->stage ? "/smem-x" : "");
+                p->stage ? "/smem-x" : "", p->pipe ? "/tma-pipe" : "");
   CK(cudaDeviceSynchronize());
   return SPARSEP_OK;
 }
@@ -389,9 +418,11 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
     for (int i = 0; i < oo.nr_parts; ++i) csr_tile_items(items, t, A->rowptr, split[i], split[i + 1], oo, true, false);
   } else {
     csr_tile_items(items, t, A->rowptr, 0, A->nrows, oo, false, true);
+    number_long_rows(items);
     for (auto &it : items) has_long |= it.kind == ITEM_LONG;
   }
   set_out_mode(p, oo, 1, has_long, 1);
+  p->pipe = !faithful && oo.lanes == 0 && p->out_mode == OUT_DIRECT && oo.nr_workers == 0;
   if ((st = upload(p, A->rowptr, (size_t)A->nrows + 1, 4, 16, (const void **)&p->rowptr))) return st;
   if ((st = upload(p, A->colind, A->nnz, 4, 16, (const void **)&p->colind))) return st;
   if ((st = upload(p, A->values, A->nnz, sizeof(T), 16, &p->val))) return st;
@@ -1170,6 +1201,7 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   P.carry_val = p->carry_w ? p->carry_val : nullptr;
   P.carry_idx = p->carry_w ? p->carry_idx : nullptr;
   P.done = p->done;
+  P.row_cnt = p->row_cnt;
   P.err = p->err;
   P.n_rowptr = p->n_rowptr;
   P.n_idx = p->n_idx;
@@ -1180,7 +1212,8 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   P.n_carry = p->carry_w ? (uint64_t)p->nitems * p->carry_w + 1 : 0;
   P.nslots = p->out_mode == OUT_PARTIAL ? p->V : 1;
   P.smem_bytes = (uint32_t)p->smem;
-  CK(launch_items<T>(P, p->format, p->carry_w, p->threads, p->smem, s));
+  if (p->pipe) CK(launch_csr_pipe<T>(P, p->sms, s, &p->pipe_grid));
+  else CK(launch_items<T>(P, p->format, p->carry_w, p->threads, p->smem, s));
   if (p->out_mode == OUT_PARTIAL) {
     CK(cudaEventRecord(p->ev[2], s));
     CK(launch_merge<T>(static_cast<const T *>(p->part), static_cast<T *>(d_y), p->nrows, p->V, p->sms, s));
