@@ -113,7 +113,9 @@ typedef struct sparsep_opts {
   int32_t lanes;           /* lanes per row / block row: 1,2,4,8,16,32; 0 = auto */
   int32_t nrhs;            /* right-hand sides (x is ncols x nrhs row-major)     */
   int32_t stage_x;         /* 2D: stage the x-segment in shared memory (1/0/-1=auto) */
-  int32_t reserved[3];
+  int32_t item_nnz;        /* auto plans: target nonzeros per CTA work item (0 = auto) */
+  int32_t pipeline;        /* 1D CSR auto plans: 1 = persistent TMA-pipelined kernel */
+  int32_t reserved[1];
 } sparsep_opts;
 
 /* Defaults: 1D, nnz balance, auto parts/workers/lanes, LF, nrhs = 1. */

@@ -23,13 +23,14 @@
 namespace sparsep {
 namespace pipe {
 
-constexpr int CAP = 4096;   // nonzeros per stage
-constexpr int RCAP = 1024;  // rows per stage
-constexpr int NT = 256;     // threads per CTA
-constexpr int PER = CAP / NT;
+constexpr int NT = 256;  // threads per CTA
 constexpr unsigned long long NO_CARRY = ~0ull;
 
-template <typename T> struct Layout {
+// CAP nonzeros / CAP/4 rows per stage; the smaller stage fits six CTAs per SM
+template <typename T, int CAP_> struct Layout {
+  static constexpr int CAP = CAP_;
+  static constexpr int RCAP = CAP_ / 4;
+  static constexpr int PER = CAP_ / NT;
   // colind and values are staged from the same element index, aligned so both
   // copies start on 16 bytes: ALIGN = max(4, 16 / sizeof(T)) elements
   static constexpr int ALIGN = (16 / (int)sizeof(T)) > 4 ? (16 / (int)sizeof(T)) : 4;
@@ -75,7 +76,7 @@ struct Win {
 
 template <typename T>
 __device__ __forceinline__ Win window(const Item &it) {
-  constexpr uint64_t VA = Layout<T>::ALIGN;
+  constexpr uint64_t VA = Layout<T, 2048>::ALIGN;
   Win w;
   if (it.kind == ITEM_LONG) {
     w.r_lo = 0;
@@ -90,10 +91,11 @@ __device__ __forceinline__ Win window(const Item &it) {
   return w;
 }
 
-template <typename T, int S>
-__global__ void __launch_bounds__(NT) csr_pipe(Params<T> P) {
+template <typename T, int S, int CAP_>
+__global__ void __launch_bounds__(NT, CAP_ <= 2048 ? 5 : 3) csr_pipe(Params<T> P) {
   using A = Acc<T>;
-  using L = Layout<T>;
+  using L = Layout<T, CAP_>;
+  constexpr int CAP = L::CAP, RCAP = L::RCAP, PER = L::PER;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t full[S];
   __shared__ A red[NT / 32];
@@ -280,17 +282,11 @@ __global__ void __launch_bounds__(NT) csr_pipe(Params<T> P) {
 // types (2 stages), 2 CTAs for the 8-byte types.
 template <typename T> constexpr int pipe_stages() { return 2; }
 
-template <typename T>
-size_t csr_pipe_smem() {
-  return pipe::Layout<T>::bytes(pipe_stages<T>());
-}
-
-template <typename T>
-cudaError_t launch_csr_pipe(const Params<T> &P, int sms, cudaStream_t st, int *grid_out) {
-  if (P.nitems == 0) return cudaSuccess;
+template <typename T, int CAP>
+static cudaError_t launch_cap(const Params<T> &P, int sms, cudaStream_t st, int *grid_out) {
   constexpr int S = pipe_stages<T>();
-  auto k = pipe::csr_pipe<T, S>;
-  const size_t smem = csr_pipe_smem<T>();
+  auto k = pipe::csr_pipe<T, S, CAP>;
+  const size_t smem = pipe::Layout<T, CAP>::bytes(S);
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -308,9 +304,17 @@ cudaError_t launch_csr_pipe(const Params<T> &P, int sms, cudaStream_t st, int *g
   return cudaGetLastError();
 }
 
+// items of at most 2048 nonzeros (and 512 rows) take the small-stage kernel
+template <typename T>
+cudaError_t launch_csr_pipe(const Params<T> &P, int sms, cudaStream_t st, int *grid_out, uint32_t max_item_nnz) {
+  if (P.nitems == 0) return cudaSuccess;
+  if (max_item_nnz <= 2048) return launch_cap<T, 2048>(P, sms, st, grid_out);
+  return launch_cap<T, 4096>(P, sms, st, grid_out);
+}
+
 #ifndef SPARSEP_KT
 #define SPARSEP_KT float
 #endif
-template cudaError_t launch_csr_pipe<SPARSEP_KT>(const Params<SPARSEP_KT> &, int, cudaStream_t, int *);
+template cudaError_t launch_csr_pipe<SPARSEP_KT>(const Params<SPARSEP_KT> &, int, cudaStream_t, int *, uint32_t);
 
 }  // namespace sparsep

@@ -274,12 +274,18 @@ __device__ void csr_long(const Params<T> &P, const Item &it, const T *__restrict
     if (SP_BAD(P, it.crow < P.nrows && (P.out_mode == OUT_ATOMIC || item_id < P.n_carry), -1007)) return;
     if (P.out_mode == OUT_ATOMIC) {
       atomic_add_out<T>(out + it.crow, tot);
-    } else if (it.chunk == 0) {
-      out[it.crow] = from_acc<T>(tot);
-      P.carry_idx[item_id] = NO_CARRY;
     } else {
+      // the last chunk of the row to arrive sums the row's partials in chunk order
       P.carry_val[item_id] = acc_bits(tot);
-      P.carry_idx[item_id] = out_index(P, it, it.crow);
+      __threadfence();
+      const unsigned int prev = atomicAdd(P.row_cnt + it.cslot, 1u);
+      if (prev == it.nchunk - 1) {
+        __threadfence();
+        A sum = A(0);
+        for (uint32_t c = 0; c < it.nchunk; ++c) sum += bits_acc<A>(__ldcg(P.carry_val + it.first + c));
+        out[it.crow] = from_acc<T>(sum);
+        P.row_cnt[it.cslot] = 0;  // ready for the next launch
+      }
     }
   }
 }
@@ -672,7 +678,6 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
         case 16: csr_rows<T, 16>(P, it, xb); break;
         default: csr_rows<T, 32>(P, it, xb); break;
       }
-      if (P.carry_idx && threadIdx.x == 0 && P.out_mode != OUT_ATOMIC) P.carry_idx[item_id] = NO_CARRY;
     }
   } else if constexpr (FMT == SPARSEP_FMT_COO) {
     elems_lf<T, 1, 0, 0>(P, it, xb, item_id, carry_w);

@@ -19,6 +19,6 @@ cudaError_t launch_merge(const T *part, T *y, uint32_t nrows, uint32_t V, int sm
 // Persistent TMA-pipelined CSR kernel (csr_pipe.cu) for 1D items built by the
 // automatic planner; grid = SMs x resident CTAs (capped at the item count).
 template <typename T>
-cudaError_t launch_csr_pipe(const Params<T> &P, int sms, cudaStream_t st, int *grid_out);
+cudaError_t launch_csr_pipe(const Params<T> &P, int sms, cudaStream_t st, int *grid_out, uint32_t max_item_nnz);
 
 }  // namespace sparsep

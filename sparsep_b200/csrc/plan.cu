@@ -52,6 +52,7 @@ struct sparsep_plan {
   bool stage = false;
   bool pipe = false;  // 1D CSR auto items run on the pipelined persistent kernel
   int pipe_grid = 0;
+  uint32_t max_item_nnz = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[5] = {};
   double t[5] = {0, 0, 0, 0, 0};
@@ -168,6 +169,11 @@ static Item make_item(const Tile &t, uint16_t kind) {
 // into LONG items when allow_long.
 static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32_t *rp, uint64_t r0, uint64_t r1,
                            const sparsep_opts &o, bool faithful, bool allow_long) {
+  // item size: <= AUTO_ITEM_NNZ nonzeros, or the option's target rounded to a
+  // stage size (2048 or 4096) less the 16 slots of copy alignment
+  const uint64_t ITEM_NNZ = (o.item_nnz > 0 && o.item_nnz <= 2048) ? 2032 : AUTO_ITEM_NNZ;
+  const uint64_t ROWS_CAP = ITEM_NNZ <= 2032 ? 512 : AUTO_ITEM_ROWS;
+  const uint64_t LONG_CHUNK = ITEM_NNZ <= 2032 ? 2048 : AUTO_LONG_CHUNK;
   auto emit = [&](uint64_t a, uint64_t b) {
     if (a >= b) return;
     Item it = make_item(t, ITEM_ROWS);
@@ -189,14 +195,14 @@ static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32
   uint64_t a = r0, acc = 0;
   for (uint64_t r = r0; r < r1; ++r) {
     uint64_t len = (uint64_t)rp[r + 1] - rp[r];
-    if (allow_long && len > AUTO_ITEM_NNZ) {
+    if (allow_long && len > ITEM_NNZ) {
       emit(a, r);
-      uint64_t nch = (len + AUTO_LONG_CHUNK - 1) / AUTO_LONG_CHUNK;
+      uint64_t nch = (len + LONG_CHUNK - 1) / LONG_CHUNK;
       const uint32_t first = (uint32_t)items.size();
       for (uint64_t c = 0; c < nch; ++c) {
         Item it = make_item(t, ITEM_LONG);
-        it.a0 = t.nnz_base + rp[r] + c * AUTO_LONG_CHUNK;
-        it.a1 = std::min<uint64_t>(t.nnz_base + rp[r + 1], it.a0 + AUTO_LONG_CHUNK);
+        it.a0 = t.nnz_base + rp[r] + c * LONG_CHUNK;
+        it.a1 = std::min<uint64_t>(t.nnz_base + rp[r + 1], it.a0 + LONG_CHUNK);
         it.crow = (uint32_t)(t.row_off + r);
         it.chunk = (uint32_t)c;
         it.n0 = it.a0;
@@ -210,7 +216,7 @@ static void csr_tile_items(std::vector<Item> &items, const Tile &t, const uint32
       acc = 0;
       continue;
     }
-    if (r > a && (acc + len > AUTO_ITEM_NNZ || r - a >= AUTO_ITEM_ROWS)) {
+    if (r > a && (acc + len > ITEM_NNZ || r - a >= ROWS_CAP)) {
       emit(a, r);
       a = r;
       acc = 0;
@@ -422,7 +428,8 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
     for (auto &it : items) has_long |= it.kind == ITEM_LONG;
   }
   set_out_mode(p, oo, 1, has_long, 1);
-  p->pipe = !faithful && oo.lanes == 0 && p->out_mode == OUT_DIRECT && oo.nr_workers == 0;
+  p->pipe = !faithful && oo.lanes == 0 && p->out_mode == OUT_DIRECT && oo.pipeline == 1;
+  for (const Item &it : items) p->max_item_nnz = std::max<uint32_t>(p->max_item_nnz, (uint32_t)(it.n1 - it.n0));
   if ((st = upload(p, A->rowptr, (size_t)A->nrows + 1, 4, 16, (const void **)&p->rowptr))) return st;
   if ((st = upload(p, A->colind, A->nnz, 4, 16, (const void **)&p->colind))) return st;
   if ((st = upload(p, A->values, A->nnz, sizeof(T), 16, &p->val))) return st;
@@ -1199,7 +1206,9 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   P.part = static_cast<T *>(p->part);
   P.out_mode = p->out_mode;
   P.carry_val = p->carry_w ? p->carry_val : nullptr;
-  P.carry_idx = p->carry_w ? p->carry_idx : nullptr;
+  // CSR long rows complete through per-row counters; the carry list and the
+  // last-CTA fix-up serve the element-wise (COO / BCOO) formats
+  P.carry_idx = (p->carry_w && p->format != SPARSEP_FMT_CSR) ? p->carry_idx : nullptr;
   P.done = p->done;
   P.row_cnt = p->row_cnt;
   P.err = p->err;
@@ -1212,7 +1221,7 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   P.n_carry = p->carry_w ? (uint64_t)p->nitems * p->carry_w + 1 : 0;
   P.nslots = p->out_mode == OUT_PARTIAL ? p->V : 1;
   P.smem_bytes = (uint32_t)p->smem;
-  if (p->pipe) CK(launch_csr_pipe<T>(P, p->sms, s, &p->pipe_grid));
+  if (p->pipe) CK(launch_csr_pipe<T>(P, p->sms, s, &p->pipe_grid, p->max_item_nnz));
   else CK(launch_items<T>(P, p->format, p->carry_w, p->threads, p->smem, s));
   if (p->out_mode == OUT_PARTIAL) {
     CK(cudaEventRecord(p->ev[2], s));
