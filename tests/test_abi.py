@@ -96,3 +96,14 @@ def test_partition_entry_points():
     assert L.sparsep_partition_by_elem(10, 3, e) == 0
     assert list(e) == [0, 4, 7, 10]
     assert L.sparsep_partition_by_row(10, 0, s) == capi.EINVAL
+
+
+@pytest.mark.parametrize("macro", ["INT8", "INT16", "INT32", "INT64", "FP32", "FP64"])
+def test_compat_header_builds_reference_style_code(tmp_path, macro):
+    """A reference-style host program (struct CSRMatrix, val_dt, -D<TYPE>)
+    compiles against include/sparsep_compat.h and links to the library."""
+    out = tmp_path / "compat"
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", f"-I{ROOT / 'include'}", f"-D{macro}",
+                        str(ROOT / "tests" / "compat_check.c"), f"-L{ROOT / 'sparsep_b200'}", "-lsparsep_b200",
+                        "-o", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
