@@ -485,6 +485,25 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
                                  const uint32_t *weights, uint32_t parts, uint32_t *split);
 
 /* ------------------------------------------------------------------------ */
+/* Allocation-free SpMV                                                      */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they multiply -- code inside a memory pool or arena that owns
+ * the device heap, or work issued between someone else's stream operations,
+ * where a cudaMalloc would synchronise the device or be refused.
+ * y = A x for a row-sorted FP32 COO matrix already on the device (d_elems:
+ * nnz reference elem_t entries, 16-byte aligned; d_x: ncols; d_y: nrows),
+ * lock-free COO kernel, stream-ordered on `stream`.  It allocates nothing:
+ * its scratch is a fixed array in the library's device image, sized for at
+ * most 2^28 nonzeros (larger inputs return SPARSEP_ERANGE), that every GPU
+ * loading the library holds until exit.  The first call on a device looks
+ * the array up (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race,
+ * so serialise them (one stream, or events). */
+int sparsep_spmv_cooe_f32_noalloc(const sparsep_elem_f32 *d_elems, uint32_t nnz, uint32_t nrows, uint32_t ncols,
+                                  const float *d_x, float *d_y, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Device information                                                        */
 /* ------------------------------------------------------------------------ */
 /* Number of SMs of the current device, or a negative status. */
