@@ -485,6 +485,46 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
                                  const uint32_t *weights, uint32_t parts, uint32_t *split);
 
 /* ------------------------------------------------------------------------ */
+/* Batched multi-RHS SpMV (no reference counterpart)                         */
+/* ------------------------------------------------------------------------ */
+/* Many CSR matrices, each with its own k = 1..256 right-hand sides (x is
+ * ncols x k and y nrows x k, row-major), multiplied by ONE persistent kernel:
+ * warps pull warp-sized row ranges of any matrix from a device work queue,
+ * replayed as a CUDA graph (queue reset + kernel).  The row routine of each
+ * matrix is a variant: mode 0 = `lanes` lanes per row over the right-hand
+ * sides (k >= 4, k <= 8*lanes), mode 1 = `lanes` lanes per row over the
+ * nonzeros (k <= 4); item_work = nonzero x RHS products per work item.
+ * FP32 and INT32 (integers wrap exactly, as the single-vector path). */
+typedef struct sparsep_batch sparsep_batch;
+typedef struct sparsep_batch_variant {
+  int32_t mode, lanes, item_work, reserved;
+} sparsep_batch_variant;
+
+void sparsep_batch_variant_default(uint32_t k, sparsep_batch_variant *v);
+int sparsep_batch_create_f32(uint32_t nmats, const sparsep_csr_f32 *const *A, const uint32_t *nrhs,
+                             const sparsep_batch_variant *variants, sparsep_batch **out);
+int sparsep_batch_create_i32(uint32_t nmats, const sparsep_csr_i32 *const *A, const uint32_t *nrhs,
+                             const sparsep_batch_variant *variants, sparsep_batch **out);
+void sparsep_batch_free(sparsep_batch *b);
+/* x / y of matrix m: device pointers, or host copies in and out */
+int sparsep_batch_x(sparsep_batch *b, uint32_t m, void **d_x, void **d_y);
+int sparsep_batch_set_x(sparsep_batch *b, uint32_t m, const void *h_x);
+int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y);
+/* change a matrix's variant; sparsep_batch_commit rebuilds the work queue */
+int sparsep_batch_set_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v);
+int sparsep_batch_commit(sparsep_batch *b);
+/* the whole batch as one graph launch (NULL stream: synchronous) */
+int sparsep_batch_execute(sparsep_batch *b, void *stream);
+/* baseline: one launch per matrix, in order */
+int sparsep_batch_execute_per_matrix(sparsep_batch *b, void *stream);
+int sparsep_batch_execute_one(sparsep_batch *b, uint32_t m, void *stream);
+/* the autotuner: every candidate variant of every matrix timed alone (median
+ * of reps), the fastest kept and committed.  times_us: nmats x candidates. */
+int sparsep_batch_candidates(sparsep_batch_variant *out, int max);
+int sparsep_batch_autotune(sparsep_batch *b, int reps, double *times_us, int32_t *chosen);
+int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free SpMV                                                      */
 /* ------------------------------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -378,3 +378,118 @@ def spmv(A: HostMatrix, x: np.ndarray, opts: Opts | None = None) -> np.ndarray:
     check(getattr(lib(), f"sparsep_spmv_{A.kind}_{A.dtype}")(A.ref, ptr(x, dt.ct), ptr(y, dt.ct), C.byref(o)),
           f"spmv_{A.kind}_{A.dtype}")
     return y
+
+
+# ---------------------------------------------------------------------------
+# batched multi-RHS SpMV
+# ---------------------------------------------------------------------------
+class BatchVariant(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("lanes", C.c_int32), ("item_work", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_tuple(self):
+        return (int(self.mode), int(self.lanes), int(self.item_work))
+
+
+def _batch_sigs(L):
+    if getattr(L, "_batch_sigs", False):
+        return
+    PB = C.c_void_p
+    for t in ("f32", "i32"):
+        f = getattr(L, f"sparsep_batch_create_{t}")
+        f.argtypes = [C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(BatchVariant), C.POINTER(C.c_void_p)]
+    L.sparsep_batch_free.argtypes = [PB]
+    L.sparsep_batch_free.restype = None
+    L.sparsep_batch_x.argtypes = [PB, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    L.sparsep_batch_set_x.argtypes = [PB, C.c_uint32, C.c_void_p]
+    L.sparsep_batch_get_y.argtypes = [PB, C.c_uint32, C.c_void_p]
+    L.sparsep_batch_set_variant.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant)]
+    L.sparsep_batch_commit.argtypes = [PB]
+    L.sparsep_batch_execute.argtypes = [PB, C.c_void_p]
+    L.sparsep_batch_execute_per_matrix.argtypes = [PB, C.c_void_p]
+    L.sparsep_batch_execute_one.argtypes = [PB, C.c_uint32, C.c_void_p]
+    L.sparsep_batch_candidates.argtypes = [C.POINTER(BatchVariant), C.c_int]
+    L.sparsep_batch_autotune.argtypes = [PB, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    L.sparsep_batch_get_info.argtypes = [PB, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.sparsep_batch_variant_default.argtypes = [C.c_uint32, C.POINTER(BatchVariant)]
+    L.sparsep_batch_variant_default.restype = None
+    L._batch_sigs = True
+
+
+def batch_candidates() -> list[BatchVariant]:
+    L = lib()
+    _batch_sigs(L)
+    n = L.sparsep_batch_candidates(None, 0)
+    arr = (BatchVariant * n)()
+    L.sparsep_batch_candidates(arr, n)
+    return list(arr)
+
+
+class Batch:
+    """Many CSR matrices with their own right-hand-side counts, one persistent launch."""
+
+    def __init__(self, dtype: str, mats: list[HostMatrix], nrhs: list[int], variants=None):
+        assert dtype in ("f32", "i32")
+        L = lib()
+        _batch_sigs(L)
+        self.dtype, self.mats, self.nrhs = dtype, mats, [int(k) for k in nrhs]
+        ptrs = (C.c_void_p * len(mats))(*[C.addressof(m.s) for m in mats])
+        ks = (C.c_uint32 * len(mats))(*self.nrhs)
+        var = None
+        if variants is not None:
+            var = (BatchVariant * len(mats))(*variants)
+        h = C.c_void_p()
+        check(getattr(L, f"sparsep_batch_create_{dtype}")(len(mats), ptrs, ks, var, C.byref(h)), "batch_create")
+        self.h = h
+        self.np = DTYPES[dtype].np
+
+    def set_x(self, m: int, x: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=self.np)
+        assert x.size == self.mats[m].s.ncols * self.nrhs[m]
+        check(lib().sparsep_batch_set_x(self.h, m, x.ctypes.data), "batch_set_x")
+
+    def get_y(self, m: int) -> np.ndarray:
+        y = np.empty((self.mats[m].s.nrows, self.nrhs[m]), dtype=self.np)
+        check(lib().sparsep_batch_get_y(self.h, m, y.ctypes.data), "batch_get_y")
+        return y
+
+    def device_xy(self, m: int):
+        dx, dy = C.c_void_p(), C.c_void_p()
+        check(lib().sparsep_batch_x(self.h, m, C.byref(dx), C.byref(dy)))
+        return dx.value, dy.value
+
+    def execute(self, stream: int | None = None):
+        check(lib().sparsep_batch_execute(self.h, C.c_void_p(stream) if stream else None), "batch_execute")
+
+    def execute_per_matrix(self, stream: int | None = None):
+        check(lib().sparsep_batch_execute_per_matrix(self.h, C.c_void_p(stream) if stream else None),
+              "batch_execute_per_matrix")
+
+    def set_variant(self, m: int, v: BatchVariant):
+        check(lib().sparsep_batch_set_variant(self.h, m, C.byref(v)), "batch_set_variant")
+
+    def commit(self):
+        check(lib().sparsep_batch_commit(self.h), "batch_commit")
+
+    def autotune(self, reps: int = 3):
+        nc = lib().sparsep_batch_candidates(None, 0)
+        t = np.zeros((len(self.mats), nc), dtype=np.float64)
+        ch = np.zeros(len(self.mats), dtype=np.int32)
+        check(lib().sparsep_batch_autotune(self.h, reps, t.ctypes.data_as(C.POINTER(C.c_double)),
+                                           ch.ctypes.data_as(C.POINTER(C.c_int32))), "batch_autotune")
+        return t, ch
+
+    def info(self):
+        b, it, nz = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().sparsep_batch_get_info(self.h, C.byref(b), C.byref(it), C.byref(nz)))
+        return dict(compulsory_bytes=b.value, items=it.value, nnz=nz.value)
+
+    def free(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().sparsep_batch_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -139,3 +139,58 @@ def bcsr_triplets(B):
     c = (B["bcolind"][:, None, None].astype(np.int64) * cb + np.arange(cb)[None, None, :]) + 0 * np.arange(rb)[None, :, None]
     m = (r < B["nrows"]) & (c < B["ncols"])
     return r[m].astype(np.uint32), c[m].astype(np.uint32), B["bval"][m]
+
+
+def stratified_cols(rng, lens, lo, hi):
+    """Per row r, lens[r] distinct sorted columns in [lo[r], hi[r]): one uniform
+    draw inside each of lens[r] equal strata (no sort, no redraw needed)."""
+    lens = np.asarray(lens, dtype=np.int64)
+    total = int(lens.sum())
+    rowptr = np.zeros(lens.size + 1, dtype=np.int64)
+    np.cumsum(lens, out=rowptr[1:])
+    row_of = np.repeat(np.arange(lens.size), lens)
+    i = np.arange(total, dtype=np.int64) - rowptr[:-1][row_of]
+    w = (hi - lo).astype(np.int64)[row_of]
+    u = rng.random(total)
+    col = lo[row_of] + np.floor((i + u) * w / lens[row_of]).astype(np.int64)
+    return rowptr.astype(np.uint32), col.astype(np.uint32)
+
+
+def batch_matrix(rng, n, kind, dtype):
+    """One square matrix of the batch workload: 'uniform' (4-64 nnz/row),
+    'zipf' (power-law row lengths, exponent 2, mean ~16) or 'banded'."""
+    lo = np.zeros(n, dtype=np.int64)
+    hi = np.full(n, n, dtype=np.int64)
+    if kind == "uniform":
+        lens = rng.integers(4, 65, n)
+    elif kind == "zipf":
+        lens = np.minimum(rng.zipf(2.0, n) * 4, min(n, 50_000))
+    else:
+        bw = int(rng.integers(8, 65))
+        r = np.arange(n)
+        lo = np.maximum(0, r - bw)
+        hi = np.minimum(n, r + bw + 1)
+        lens = np.minimum(hi - lo, rng.integers(4, 65, n))
+    lens = np.minimum(lens, hi - lo)
+    rowptr, cols = stratified_cols(rng, lens, lo, hi)
+    dt = np.dtype(dtype)
+    vals = rng.uniform(-1, 1, cols.size).astype(dt) if dt.kind == "f" else rng.integers(-8, 9, cols.size).astype(dt)
+    return rowptr, cols, vals
+
+
+def batch_workload(nmats=512, seed=3, dtype=np.float32, rows_lo=1_000, rows_hi=256_000, k_max=32):
+    """The batched workload: nmats square matrices, rows log-uniform in
+    [rows_lo, rows_hi], a mix of uniform / Zipf / banded structure, each with
+    1..k_max right-hand sides (x uniform in [-1, 1], integers in [-8, 8])."""
+    rng = np.random.default_rng(seed)
+    out = []
+    kinds = ("uniform", "zipf", "banded")
+    for m in range(nmats):
+        n = int(np.exp(rng.uniform(np.log(rows_lo), np.log(rows_hi))))
+        kind = kinds[m % 3]
+        k = int(rng.integers(1, k_max + 1))
+        rowptr, cols, vals = batch_matrix(rng, n, kind, dtype)
+        dt = np.dtype(dtype)
+        x = rng.uniform(-1, 1, (n, k)).astype(dt) if dt.kind == "f" else rng.integers(-8, 9, (n, k)).astype(dt)
+        out.append(dict(n=n, kind=kind, k=k, rowptr=rowptr, colind=cols, values=vals, x=x))
+    return out
