@@ -53,29 +53,44 @@ __device__ __forceinline__ void rows_rhs(const Mat<T> &m, uint32_t r0, uint32_t 
   using A = Acc<T>;
   constexpr int NG = 32 / G;
   const int g = lane / G, gl = lane % G;
+  // shuffles stay inside the group: its lanes share a row, hence a trip count
+  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (g * G));
   for (uint32_t base = r0; base < r1; base += NG) {
     const uint32_t r = base + g;
-    if (r < r1) {
-      A acc[ACC_RHS];
+    if (r >= r1) continue;
+    A acc[ACC_RHS];
 #pragma unroll
-      for (int a = 0; a < ACC_RHS; ++a) acc[a] = A(0);
-      const uint32_t s = __ldg(m.rowptr + r), e = __ldg(m.rowptr + r + 1);
-      for (uint32_t p = s; p < e; ++p) {
-        const uint32_t c = __ldcs(m.colind + p);
-        const T v = __ldcs(m.val + p);
-        const T *xr = m.x + (size_t)c * m.k;
+    for (int a = 0; a < ACC_RHS; ++a) acc[a] = A(0);
+    const uint32_t s = __ldg(m.rowptr + r), e = __ldg(m.rowptr + r + 1);
+    for (uint32_t p0 = s; p0 < e; p0 += G) {
+      // the group loads G nonzeros at once, then every lane walks them with
+      // all of their x loads independent of each other
+      uint32_t cl = 0;
+      T vl = T(0);
+      if (p0 + gl < e) {
+        cl = __ldcs(m.colind + p0 + gl);
+        vl = __ldcs(m.val + p0 + gl);
+      }
+      const uint32_t cnt = e - p0 < (uint32_t)G ? e - p0 : (uint32_t)G;
 #pragma unroll
-        for (int a = 0; a < ACC_RHS; ++a) {
-          const uint32_t j = gl + a * G;
-          if (j < m.k) acc[a] += mul<T>(v, __ldg(xr + j));
+      for (int q = 0; q < G; ++q) {
+        if ((uint32_t)q < cnt) {
+          const uint32_t c = __shfl_sync(gmask, cl, q, G);
+          const T v = __shfl_sync(gmask, vl, q, G);
+          const T *xr = m.x + (size_t)c * m.k;
+#pragma unroll
+          for (int a = 0; a < ACC_RHS; ++a) {
+            const uint32_t j = gl + a * G;
+            if (j < m.k) acc[a] += mul<T>(v, __ldg(xr + j));
+          }
         }
       }
-      T *yr = m.y + (size_t)r * m.k;
+    }
+    T *yr = m.y + (size_t)r * m.k;
 #pragma unroll
-      for (int a = 0; a < ACC_RHS; ++a) {
-        const uint32_t j = gl + a * G;
-        if (j < m.k) yr[j] = from_acc<T>(acc[a]);
-      }
+    for (int a = 0; a < ACC_RHS; ++a) {
+      const uint32_t j = gl + a * G;
+      if (j < m.k) yr[j] = from_acc<T>(acc[a]);
     }
   }
 }
@@ -93,6 +108,7 @@ __device__ __forceinline__ void rows_nnz(const Mat<T> &m, uint32_t r0, uint32_t 
     for (int a = 0; a < KMAX_NNZ_MODE; ++a) acc[a] = A(0);
     if (ok) {
       const uint32_t s = __ldg(m.rowptr + r), e = __ldg(m.rowptr + r + 1);
+#pragma unroll 4
       for (uint32_t p = s + gl; p < e; p += G) {
         const uint32_t c = __ldcs(m.colind + p);
         const T v = __ldcs(m.val + p);
@@ -219,7 +235,7 @@ static void make_items(sparsep_batch *b, uint32_t m, const uint32_t *rowptr) {
   const auto &M = b->mats_h[m];
   const sparsep_batch_variant &v = b->var[m];
   b->item0[m] = (uint32_t)b->items_h.size();
-  const uint64_t target = v.item_work > 0 ? (uint64_t)v.item_work : 4096;
+  const uint64_t target = v.item_work > 0 ? (uint64_t)v.item_work : 16384;
   const uint32_t rows_min = v.mode == 0 ? 32 / v.lanes : 32 / v.lanes;
   uint32_t r = 0;
   while (r < M.nrows) {
@@ -265,7 +281,7 @@ extern "C" void sparsep_batch_variant_default(uint32_t k, sparsep_batch_variant 
     v->mode = 1;
     v->lanes = 8;
   }
-  v->item_work = 4096;
+  v->item_work = 16384;
 }
 
 template <typename T>
@@ -501,9 +517,10 @@ int sparsep_batch_execute_one(sparsep_batch *b, uint32_t m, void *stream) {
 // times_us (nmats x sparsep_batch_candidates()) receives the medians, 0 for
 // candidates that do not apply to a matrix; chosen (nmats) the chosen index.
 static const sparsep_batch_variant kCand[] = {
-    {0, 4, 2048, 0},  {0, 8, 2048, 0},  {0, 16, 2048, 0}, {0, 32, 2048, 0}, {0, 4, 8192, 0},  {0, 8, 8192, 0},
-    {0, 16, 8192, 0}, {0, 32, 8192, 0}, {1, 1, 2048, 0},  {1, 2, 2048, 0},  {1, 4, 2048, 0},  {1, 8, 2048, 0},
-    {1, 16, 2048, 0}, {1, 32, 2048, 0}, {1, 1, 8192, 0},  {1, 4, 8192, 0},  {1, 8, 8192, 0},  {1, 32, 8192, 0}};
+    {0, 4, 16384, 0},  {0, 8, 16384, 0},  {0, 16, 16384, 0},  {0, 32, 16384, 0}, {0, 4, 131072, 0},
+    {0, 8, 131072, 0}, {0, 16, 131072, 0}, {0, 32, 131072, 0}, {1, 1, 16384, 0},  {1, 2, 16384, 0},
+    {1, 4, 16384, 0},  {1, 8, 16384, 0},  {1, 16, 16384, 0},  {1, 32, 16384, 0}, {1, 1, 131072, 0},
+    {1, 4, 131072, 0}, {1, 8, 131072, 0}, {1, 32, 131072, 0}};
 constexpr int kNCand = sizeof(kCand) / sizeof(kCand[0]);
 
 int sparsep_batch_candidates(sparsep_batch_variant *out, int max) {
