@@ -488,16 +488,22 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
 /* Batched multi-RHS SpMV (no reference counterpart)                         */
 /* ------------------------------------------------------------------------ */
 /* Many CSR matrices, each with its own k = 1..256 right-hand sides (x is
- * ncols x k and y nrows x k, row-major), multiplied by ONE persistent kernel:
- * warps pull warp-sized row ranges of any matrix from a device work queue,
- * replayed as a CUDA graph (queue reset + kernel).  The row routine of each
- * matrix is a variant: mode 0 = `lanes` lanes per row over the right-hand
- * sides (k >= 4, k <= 8*lanes), mode 1 = `lanes` lanes per row over the
- * nonzeros (k <= 4); item_work = nonzero x RHS products per work item.
- * FP32 and INT32 (integers wrap exactly, as the single-vector path). */
+ * ncols x k and y nrows x k, row-major), multiplied by ONE kernel launch:
+ * its CTAs claim work items (row ranges of any matrix, at most 2048 nonzeros,
+ * or one longer row) from a device work queue by atomic ticket, replayed as a
+ * CUDA graph (queue reset + kernel).  The row routine of each matrix is a
+ * variant: the CTA is cut into groups of `lanes` (1..32, power of two) lanes,
+ * each lane reading `vec` (1, 2, 4; k % vec == 0) consecutive right-hand
+ * sides per load, k <= 8 * lanes;
+ *   mode 0: the rows of a work item dealt round-robin to the groups;
+ *   mode 1: the rows and nonzeros of a work item split evenly over the groups
+ *           (merge path), rows cut by a split finished from carries;
+ *   item_work: nonzero x right-hand-side products per item (0 = 16384).
+ * FP32 and INT32 (integers wrap exactly, as the single-vector path).  Status
+ * ENOSYS: the variant does not apply to that k. */
 typedef struct sparsep_batch sparsep_batch;
 typedef struct sparsep_batch_variant {
-  int32_t mode, lanes, item_work, reserved;
+  int32_t mode, lanes, item_work, vec;
 } sparsep_batch_variant;
 
 void sparsep_batch_variant_default(uint32_t k, sparsep_batch_variant *v);
@@ -512,16 +518,31 @@ int sparsep_batch_set_x(sparsep_batch *b, uint32_t m, const void *h_x);
 int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y);
 /* change a matrix's variant; sparsep_batch_commit rebuilds the work queue */
 int sparsep_batch_set_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v);
+int sparsep_batch_get_variant(const sparsep_batch *b, uint32_t m, sparsep_batch_variant *v);
 int sparsep_batch_commit(sparsep_batch *b);
-/* the whole batch as one graph launch (NULL stream: synchronous) */
+/* the whole batch as one graph launch (NULL stream: synchronous, and the
+ * status of sparsep_batch_status is returned) */
 int sparsep_batch_execute(sparsep_batch *b, void *stream);
-/* baseline: one launch per matrix, in order */
+/* SPARSEP_ETIMEDOUT if a work item's staging copy did not land within its
+ * bounded wait since the last call (that item's rows were not written), else
+ * OK; waits for the batch's work */
+int sparsep_batch_status(sparsep_batch *b);
+/* 1 (default): the batch launch's CTAs claim work items by atomic ticket, so
+ * items start in queue order (long rows first); 0: CTA b runs item b */
+int sparsep_batch_set_ticket(sparsep_batch *b, int on);
+/* baseline: one plain launch per matrix, in order, each with the default
+ * variant for its k and items sized to spread over all SMs */
 int sparsep_batch_execute_per_matrix(sparsep_batch *b, void *stream);
+/* one matrix alone with its committed items */
 int sparsep_batch_execute_one(sparsep_batch *b, uint32_t m, void *stream);
 /* the autotuner: every candidate variant of every matrix timed alone (median
- * of reps), the fastest kept and committed.  times_us: nmats x candidates. */
+ * of reps), the fastest kept and committed.  times_us: nmats x candidates,
+ * 0 where a candidate does not apply. */
 int sparsep_batch_candidates(sparsep_batch_variant *out, int max);
 int sparsep_batch_autotune(sparsep_batch *b, int reps, double *times_us, int32_t *chosen);
+/* median time of matrix m alone under variant v (ENOSYS: not applicable) */
+int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v, int reps,
+                               double *us_out);
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
 
 /* ------------------------------------------------------------------------ */

@@ -1,7 +1,8 @@
 """Build libsparsep_b200.so in-tree with nvcc for sm_100a.
 
-Sources: csrc/kernels.cu (compiled once per element type, in parallel),
-csrc/plan.cu and csrc/formats.cpp.  Objects go to sparsep_b200/_build/.
+Sources: csrc/kernels.cu and csrc/csr_pipe.cu (compiled once per element
+type, in parallel), csrc/batch_kernels.cu (once per batched type), the other
+csrc/*.cu and csrc/*.cpp.  Objects go to sparsep_b200/_build/.
 """
 from __future__ import annotations
 
@@ -22,6 +23,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
               f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 KERNEL_TYPES = {"i8": "int8_t", "i16": "int16_t", "i32": "int32_t", "i64": "int64_t",
                 "f32": "float", "f64": "double"}
+BATCH_TYPES = ("f32", "i32")
 
 
 def nvcc() -> str:
@@ -62,12 +64,17 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
     flags = NVCC_FLAGS + (["-DSPARSEP_CHECK"] if checked else [])
     jobs = []
     objs = []
-    per_type = ("kernels.cu", "csr_pipe.cu")
+    per_type = ("kernels.cu", "csr_pipe.cu", "batch_kernels.cu")
     for tag, ctype in KERNEL_TYPES.items():
-        for name in per_type:
+        for name in per_type[:2]:
             o = bdir / f"{Path(name).stem}_{tag}.o"
             objs.append(o)
             jobs.append([nvcc(), *ARCH, *flags, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / name), "-o", str(o)])
+    for tag in BATCH_TYPES:  # the batched path: FP32 and INT32
+        o = bdir / f"batch_kernels_{tag}.o"
+        objs.append(o)
+        jobs.append([nvcc(), *ARCH, *flags, f"-DSPARSEP_BT={KERNEL_TYPES[tag]}", "-c",
+                     str(CSRC / "batch_kernels.cu"), "-o", str(o)])
     for src in sorted(CSRC.glob("*.cu")):
         if src.name in per_type:
             continue

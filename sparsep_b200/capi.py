@@ -384,10 +384,21 @@ def spmv(A: HostMatrix, x: np.ndarray, opts: Opts | None = None) -> np.ndarray:
 # batched multi-RHS SpMV
 # ---------------------------------------------------------------------------
 class BatchVariant(C.Structure):
-    _fields_ = [("mode", C.c_int32), ("lanes", C.c_int32), ("item_work", C.c_int32), ("reserved", C.c_int32)]
+    _fields_ = [("mode", C.c_int32), ("lanes", C.c_int32), ("item_work", C.c_int32), ("vec", C.c_int32)]
 
     def as_tuple(self):
-        return (int(self.mode), int(self.lanes), int(self.item_work))
+        return (int(self.mode), int(self.lanes), int(self.item_work), int(self.vec))
+
+    def applies(self, k: int) -> bool:
+        """Whether this variant can run a matrix with k right-hand sides."""
+        v = max(1, int(self.vec))
+        if k % v:
+            return False
+        per = -(-k // (self.lanes * v))
+        acc = 1
+        while acc < per:
+            acc *= 2
+        return acc * v <= 8
 
 
 def _batch_sigs(L):
@@ -403,8 +414,13 @@ def _batch_sigs(L):
     L.sparsep_batch_set_x.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_get_y.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_set_variant.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant)]
+    L.sparsep_batch_get_variant.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant)]
+    L.sparsep_batch_time_variant.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant), C.c_int,
+                                             C.POINTER(C.c_double)]
     L.sparsep_batch_commit.argtypes = [PB]
     L.sparsep_batch_execute.argtypes = [PB, C.c_void_p]
+    L.sparsep_batch_status.argtypes = [PB]
+    L.sparsep_batch_set_ticket.argtypes = [PB, C.c_int]
     L.sparsep_batch_execute_per_matrix.argtypes = [PB, C.c_void_p]
     L.sparsep_batch_execute_one.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_candidates.argtypes = [C.POINTER(BatchVariant), C.c_int]
@@ -464,8 +480,29 @@ class Batch:
         check(lib().sparsep_batch_execute_per_matrix(self.h, C.c_void_p(stream) if stream else None),
               "batch_execute_per_matrix")
 
+    def status(self):
+        """Raise if a work item's staging copy timed out since the last check."""
+        check(lib().sparsep_batch_status(self.h), "batch_status")
+
+    def set_ticket(self, on: bool):
+        check(lib().sparsep_batch_set_ticket(self.h, int(bool(on))), "batch_set_ticket")
+
     def set_variant(self, m: int, v: BatchVariant):
         check(lib().sparsep_batch_set_variant(self.h, m, C.byref(v)), "batch_set_variant")
+
+    def get_variant(self, m: int) -> BatchVariant:
+        v = BatchVariant()
+        check(lib().sparsep_batch_get_variant(self.h, m, C.byref(v)), "batch_get_variant")
+        return v
+
+    def time_variant(self, m: int, v: BatchVariant, reps: int = 3) -> float | None:
+        """Median microseconds of matrix m alone under v; None if v does not apply."""
+        us = C.c_double()
+        st = lib().sparsep_batch_time_variant(self.h, m, C.byref(v), reps, C.byref(us))
+        if st == ENOSYS:
+            return None
+        check(st, "batch_time_variant")
+        return us.value
 
     def commit(self):
         check(lib().sparsep_batch_commit(self.h), "batch_commit")

@@ -1,20 +1,7 @@
-// batch.cu -- many CSR matrices with 1..32 right-hand sides in one persistent
-// launch, fed by a device work queue and replayed as a CUDA graph.
-//
-// Each matrix m has its own device copy (rowptr, colind, values), its x
-// (ncols x k, row-major) and y (nrows x k).  Work items are row ranges of one
-// matrix sized for one warp; persistent warps pull items from a global counter
-// (atomicAdd, no waiting) until the queue is empty, so matrices of very
-// different sizes share the GPU without per-matrix launch gaps or tails.
-//
-// Two row routines, chosen per matrix (the autotuner picks `lanes`):
-//   RHS mode (k >= 4): a group of G lanes per row, lane j holds right-hand
-//     sides j, j+G, ...; each nonzero's x row x[c*k .. c*k+k) is one coalesced
-//     load across the group.
-//   NNZ mode: a group of G lanes per row splits the row's nonzeros, each lane
-//     keeps k (<= 4) partial sums, then a shuffle reduction over the group.
-// Same arithmetic as the single-vector path: integers accumulate in 32/64-bit
-// unsigned and wrap exactly; FP in the element type.
+// batch.cu -- host side of the batched multi-RHS SpMV: device copies of the
+// matrices, work items and their queue order, the graph-captured batch
+// launch, the per-matrix baseline and the exhaustive variant autotuner.  The
+// kernels are in batch_kernels.cu.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -23,164 +10,8 @@
 #include <new>
 #include <vector>
 
-#include "device.cuh"
+#include "batch.hpp"
 #include "internal.hpp"
-
-namespace sparsep {
-namespace batch {
-
-template <typename T> struct Mat {
-  const uint32_t *rowptr;
-  const uint32_t *colind;
-  const T *val;
-  const T *x;
-  T *y;
-  uint32_t nrows, ncols, k, pad;
-};
-
-struct BItem {
-  uint32_t mat;
-  uint32_t r0, r1;
-  uint16_t lanes;  // G
-  uint16_t mode;   // 0 = lanes over right-hand sides, 1 = lanes over nonzeros
-};
-
-constexpr int KMAX_NNZ_MODE = 4;  // right-hand sides per lane in NNZ mode
-constexpr int ACC_RHS = 8;        // accumulators per lane in RHS mode (k <= 8 * G)
-
-template <typename T, int G>
-__device__ __forceinline__ void rows_rhs(const Mat<T> &m, uint32_t r0, uint32_t r1, int lane) {
-  using A = Acc<T>;
-  constexpr int NG = 32 / G;
-  const int g = lane / G, gl = lane % G;
-  // shuffles stay inside the group: its lanes share a row, hence a trip count
-  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (g * G));
-  for (uint32_t base = r0; base < r1; base += NG) {
-    const uint32_t r = base + g;
-    if (r >= r1) continue;
-    A acc[ACC_RHS];
-#pragma unroll
-    for (int a = 0; a < ACC_RHS; ++a) acc[a] = A(0);
-    const uint32_t s = __ldg(m.rowptr + r), e = __ldg(m.rowptr + r + 1);
-    for (uint32_t p0 = s; p0 < e; p0 += G) {
-      // the group loads G nonzeros at once, then every lane walks them with
-      // all of their x loads independent of each other
-      uint32_t cl = 0;
-      T vl = T(0);
-      if (p0 + gl < e) {
-        cl = __ldcs(m.colind + p0 + gl);
-        vl = __ldcs(m.val + p0 + gl);
-      }
-      const uint32_t cnt = e - p0 < (uint32_t)G ? e - p0 : (uint32_t)G;
-#pragma unroll
-      for (int q = 0; q < G; ++q) {
-        if ((uint32_t)q < cnt) {
-          const uint32_t c = __shfl_sync(gmask, cl, q, G);
-          const T v = __shfl_sync(gmask, vl, q, G);
-          const T *xr = m.x + (size_t)c * m.k;
-#pragma unroll
-          for (int a = 0; a < ACC_RHS; ++a) {
-            const uint32_t j = gl + a * G;
-            if (j < m.k) acc[a] += mul<T>(v, __ldg(xr + j));
-          }
-        }
-      }
-    }
-    T *yr = m.y + (size_t)r * m.k;
-#pragma unroll
-    for (int a = 0; a < ACC_RHS; ++a) {
-      const uint32_t j = gl + a * G;
-      if (j < m.k) yr[j] = from_acc<T>(acc[a]);
-    }
-  }
-}
-
-template <typename T, int G>
-__device__ __forceinline__ void rows_nnz(const Mat<T> &m, uint32_t r0, uint32_t r1, int lane) {
-  using A = Acc<T>;
-  constexpr int NG = 32 / G;
-  const int g = lane / G, gl = lane % G;
-  for (uint32_t base = r0; base < r1; base += NG) {
-    const uint32_t r = base + g;
-    const bool ok = r < r1;
-    A acc[KMAX_NNZ_MODE];
-#pragma unroll
-    for (int a = 0; a < KMAX_NNZ_MODE; ++a) acc[a] = A(0);
-    if (ok) {
-      const uint32_t s = __ldg(m.rowptr + r), e = __ldg(m.rowptr + r + 1);
-#pragma unroll 4
-      for (uint32_t p = s + gl; p < e; p += G) {
-        const uint32_t c = __ldcs(m.colind + p);
-        const T v = __ldcs(m.val + p);
-        const T *xr = m.x + (size_t)c * m.k;
-#pragma unroll
-        for (int a = 0; a < KMAX_NNZ_MODE; ++a)
-          if (a < (int)m.k) acc[a] += mul<T>(v, __ldg(xr + a));
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < KMAX_NNZ_MODE; ++a)
-#pragma unroll
-      for (int o = G / 2; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
-    if (ok && gl == 0) {
-      T *yr = m.y + (size_t)r * m.k;
-#pragma unroll
-      for (int a = 0; a < KMAX_NNZ_MODE; ++a)
-        if (a < (int)m.k) yr[a] = from_acc<T>(acc[a]);
-    }
-  }
-}
-
-template <typename T>
-__device__ void run_item(const Mat<T> &m, const BItem &it, int lane) {
-  if (it.mode == 0) {
-    switch (it.lanes) {
-      case 4: rows_rhs<T, 4>(m, it.r0, it.r1, lane); break;
-      case 8: rows_rhs<T, 8>(m, it.r0, it.r1, lane); break;
-      case 16: rows_rhs<T, 16>(m, it.r0, it.r1, lane); break;
-      default: rows_rhs<T, 32>(m, it.r0, it.r1, lane); break;
-    }
-  } else {
-    switch (it.lanes) {
-      case 1: rows_nnz<T, 1>(m, it.r0, it.r1, lane); break;
-      case 2: rows_nnz<T, 2>(m, it.r0, it.r1, lane); break;
-      case 4: rows_nnz<T, 4>(m, it.r0, it.r1, lane); break;
-      case 8: rows_nnz<T, 8>(m, it.r0, it.r1, lane); break;
-      case 16: rows_nnz<T, 16>(m, it.r0, it.r1, lane); break;
-      default: rows_nnz<T, 32>(m, it.r0, it.r1, lane); break;
-    }
-  }
-}
-
-// Persistent: every warp takes items from the queue until it is empty.
-template <typename T>
-__global__ void __launch_bounds__(256) persistent(const Mat<T> *mats, const BItem *items, uint32_t nitems,
-                                                  unsigned int *head) {
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    unsigned int i = 0;
-    if (lane == 0) i = atomicAdd(head, 1u);
-    i = __shfl_sync(0xffffffffu, i, 0);
-    if (i >= nitems) break;
-    const BItem it = items[i];
-    const Mat<T> m = mats[it.mat];
-    run_item<T>(m, it, lane);
-  }
-}
-
-// One matrix, one warp per item, no queue (the per-matrix launches and the
-// autotuner's timing runs).
-template <typename T>
-__global__ void __launch_bounds__(256) per_matrix(const Mat<T> *mats, const BItem *items, uint32_t i0, uint32_t n) {
-  const uint32_t w = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  if (w >= n) return;
-  const BItem it = items[i0 + w];
-  const Mat<T> m = mats[it.mat];
-  run_item<T>(m, it, threadIdx.x & 31);
-}
-
-}  // namespace batch
-}  // namespace sparsep
 
 using namespace sparsep;
 using namespace sparsep::batch;
@@ -193,23 +24,29 @@ struct sparsep_batch {
   std::vector<void *> allocs;
   std::vector<Mat<float>> mats_h;  // pointers are type-agnostic; values reinterpreted per dtype
   std::vector<uint64_t> nnz;
+  std::vector<std::vector<uint32_t>> rowptr;  // host copies: items are rebuilt without a read-back
   std::vector<sparsep_batch_variant> var;
-  std::vector<BItem> items_h;
+  std::vector<BItem> items_h;          // committed items, matrix after matrix
   std::vector<uint32_t> item0, nitem;  // per matrix: first item and count
-  void *mats_d = nullptr;
-  BItem *items_d = nullptr;
+  std::vector<BItem> base_h;           // the per-matrix baseline's items
+  std::vector<uint32_t> base0, nbase;
+  int *err = nullptr;  // staging timeouts (SPARSEP_ETIMEDOUT), sticky until read
+  bool ticket = true;  // batch launch: CTAs claim items by atomic ticket (else CTA b runs item b)
+  BItem *items_d = nullptr;  // committed items (per-matrix launches of one matrix)
+  BItem *queue_d = nullptr;  // the same items in queue order (long rows first)
+  BItem *base_d = nullptr;
   unsigned int *head = nullptr;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t bytes = 0;  // compulsory bytes of one batch execution
-  int grid = 0;
 };
 
-static thread_local char g_batch_err[256] = "";
 static int bmap(cudaError_t e) {
   if (e == cudaSuccess) return SPARSEP_OK;
-  std::snprintf(g_batch_err, sizeof g_batch_err, "%s (%d)", cudaGetErrorString(e), (int)e);
+  char msg[256];
+  std::snprintf(msg, sizeof msg, "%s (%d)", cudaGetErrorString(e), (int)e);
+  sparsep::record_error(msg);
   if (e == cudaErrorMemoryAllocation) return SPARSEP_ENOMEM;
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
     return SPARSEP_ENODEV;
@@ -229,59 +66,155 @@ static int balloc(sparsep_batch *b, size_t bytes, void **out) {
   return SPARSEP_OK;
 }
 
-// Items of one matrix for a variant: warp-sized row ranges holding about
-// `target` nonzero x right-hand-side products.
-static void make_items(sparsep_batch *b, uint32_t m, const uint32_t *rowptr) {
-  const auto &M = b->mats_h[m];
-  const sparsep_batch_variant &v = b->var[m];
-  b->item0[m] = (uint32_t)b->items_h.size();
-  const uint64_t target = v.item_work > 0 ? (uint64_t)v.item_work : 16384;
-  const uint32_t rows_min = v.mode == 0 ? 32 / v.lanes : 32 / v.lanes;
-  uint32_t r = 0;
-  while (r < M.nrows) {
-    uint32_t r1 = r;
-    uint64_t work = 0;
-    do {
-      const uint32_t end = std::min(M.nrows, r1 + rows_min);
-      work += ((uint64_t)rowptr[end] - rowptr[r1] + (end - r1)) * M.k;
-      r1 = end;
-    } while (r1 < M.nrows && work < target);
-    BItem it;
-    it.mat = m;
-    it.r0 = r;
-    it.r1 = r1;
-    it.lanes = (uint16_t)v.lanes;
-    it.mode = (uint16_t)v.mode;
-    b->items_h.push_back(it);
-    r = r1;
+static void bfree(sparsep_batch *b, void *d) {
+  if (!d) return;
+  for (auto i = b->allocs.begin(); i != b->allocs.end(); ++i)
+    if (*i == d) {
+      cudaFree(*i);
+      b->allocs.erase(i);
+      return;
+    }
+}
+
+static uint32_t pow2ceil(uint32_t v) {
+  uint32_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+static constexpr uint32_t DEFAULT_ITEM_WORK = 16384;  // nonzero x right-hand-side products per item
+
+// Nonzeros per item for a variant: about item_work products, within [32, BCAP].
+static uint32_t item_cap(const sparsep_batch_variant &v, uint32_t k) {
+  const uint64_t w = v.item_work > 0 ? (uint64_t)v.item_work : DEFAULT_ITEM_WORK;
+  return (uint32_t)std::min<uint64_t>(BCAP, std::max<uint64_t>(32, w / k));
+}
+
+// Items of one matrix: consecutive rows up to `cap` nonzeros and BRCAP rows;
+// a row longer than BCAP is an item of its own (processed in chunks).
+static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparsep_batch_variant &v,
+                       uint32_t cap, std::vector<BItem> &out) {
+  const uint32_t k = M.k;
+  const uint32_t V = (uint32_t)std::max(1, v.vec);
+  const uint32_t acc = pow2ceil((k + v.lanes * V - 1) / (v.lanes * V));
+  const uint32_t g_long = std::min<uint32_t>(32, pow2ceil(k));
+  const uint32_t acc_long = pow2ceil((k + g_long - 1) / g_long);
+  BItem base{};
+  base.rowptr = M.rowptr;
+  base.colind = M.colind;
+  base.val = M.val;
+  base.x = M.x;
+  base.y = M.y;
+  base.k = k;
+  BItem cur{};
+  bool open = false;
+  auto flush = [&]() {
+    if (open) out.push_back(cur);
+    open = false;
+  };
+  for (uint32_t r = 0; r < M.nrows; ++r) {
+    const uint32_t len = rowptr[r + 1] - rowptr[r];
+    if (len > BCAP) {
+      flush();
+      BItem it = base;
+      it.r0 = r;
+      it.r1 = r + 1;
+      it.p0 = rowptr[r];
+      it.p1 = rowptr[r + 1];
+      it.mode = MODE_LONG;
+      it.lanes = (uint8_t)g_long;
+      it.vec = 1;
+      it.acc = (uint8_t)acc_long;
+      out.push_back(it);
+      continue;
+    }
+    if (open && (cur.p1 - cur.p0 + len > cap || cur.r1 - cur.r0 == BRCAP)) flush();
+    if (!open) {
+      cur = base;
+      cur.r0 = cur.r1 = r;
+      cur.p0 = cur.p1 = rowptr[r];
+      cur.mode = v.mode == 0 ? MODE_ROWS : MODE_MERGE;
+      cur.lanes = (uint8_t)v.lanes;
+      cur.vec = (uint8_t)V;
+      cur.acc = (uint8_t)acc;
+      open = true;
+    }
+    cur.r1 = r + 1;
+    cur.p1 = rowptr[r + 1];
   }
-  b->nitem[m] = (uint32_t)b->items_h.size() - b->item0[m];
+  flush();
 }
 
 static int check_variant(const sparsep_batch_variant &v, uint32_t k) {
-  if (v.mode == 0) {
-    if (v.lanes != 4 && v.lanes != 8 && v.lanes != 16 && v.lanes != 32) return SPARSEP_EINVAL;
-    if (k > (uint32_t)ACC_RHS * v.lanes) return SPARSEP_ENOSYS;
-  } else if (v.mode == 1) {
-    if (v.lanes < 1 || v.lanes > 32 || (v.lanes & (v.lanes - 1))) return SPARSEP_EINVAL;
-    if (k > (uint32_t)KMAX_NNZ_MODE) return SPARSEP_ENOSYS;
-  } else {
-    return SPARSEP_EINVAL;
+  if (v.item_work < 0 || (v.mode != 0 && v.mode != 1)) return SPARSEP_EINVAL;
+  const int V = v.vec ? v.vec : 1;
+  if (v.lanes < 1 || v.lanes > 32 || (v.lanes & (v.lanes - 1))) return SPARSEP_EINVAL;
+  if (V != 1 && V != 2 && V != 4) return SPARSEP_EINVAL;
+  if (k % V) return SPARSEP_ENOSYS;
+  if (pow2ceil((k + v.lanes * V - 1) / (v.lanes * V)) * V > (uint32_t)ACC_REGS) return SPARSEP_ENOSYS;
+  return SPARSEP_OK;
+}
+
+// Merge mode, the widest vector load that divides k, and enough lanes for
+// one pass over the right-hand sides (at most 32).
+extern "C" void sparsep_batch_variant_default(uint32_t k, sparsep_batch_variant *v) {
+  if (!v) return;
+  std::memset(v, 0, sizeof *v);
+  v->mode = 1;
+  v->vec = k % 4 == 0 ? 4 : (k % 2 == 0 ? 2 : 1);
+  v->lanes = (int)std::min<uint32_t>(32, pow2ceil((k + v->vec - 1) / v->vec));
+  while (check_variant(*v, k) && v->vec > 1) {
+    v->vec >>= 1;
+    v->lanes = (int)std::min<uint32_t>(32, pow2ceil((k + v->vec - 1) / v->vec));
+  }
+  v->item_work = 0;
+}
+
+// Queue order of the batch launch: long-row items first (largest
+// first), then the rest matrix after matrix.
+static void queue_order(const std::vector<BItem> &in, std::vector<BItem> &q) {
+  q.clear();
+  q.reserve(in.size());
+  for (const BItem &it : in)
+    if (it.mode == MODE_LONG) q.push_back(it);
+  std::stable_sort(q.begin(), q.end(), [](const BItem &a, const BItem &b) { return a.p1 - a.p0 > b.p1 - b.p0; });
+  for (const BItem &it : in)
+    if (it.mode != MODE_LONG) q.push_back(it);
+}
+
+// Committed variants -> items, queue, device copies; drops the captured graph.
+static int rebuild(sparsep_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->items_h.clear();
+  for (uint32_t m = 0; m < b->nmats; ++m) {
+    b->item0[m] = (uint32_t)b->items_h.size();
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->var[m], item_cap(b->var[m], b->mats_h[m].k), b->items_h);
+    b->nitem[m] = (uint32_t)b->items_h.size() - b->item0[m];
+  }
+  std::vector<BItem> q;
+  queue_order(b->items_h, q);
+  bfree(b, b->items_d);
+  bfree(b, b->queue_d);
+  b->items_d = b->queue_d = nullptr;
+  const size_t bytes = sizeof(BItem) * std::max<size_t>(1, b->items_h.size());
+  int st = balloc(b, bytes, (void **)&b->items_d);
+  if (!st) st = balloc(b, bytes, (void **)&b->queue_d);
+  if (st) return st;
+  if (!b->items_h.empty()) {
+    BCK(cudaMemcpy(b->items_d, b->items_h.data(), sizeof(BItem) * b->items_h.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(b->queue_d, q.data(), sizeof(BItem) * q.size(), cudaMemcpyHostToDevice));
   }
   return SPARSEP_OK;
 }
 
-extern "C" void sparsep_batch_variant_default(uint32_t k, sparsep_batch_variant *v) {
-  if (!v) return;
-  std::memset(v, 0, sizeof *v);
-  if (k >= 4) {
-    v->mode = 0;
-    v->lanes = k >= 32 ? 32 : (k >= 16 ? 16 : (k >= 8 ? 8 : 4));
-  } else {
-    v->mode = 1;
-    v->lanes = 8;
-  }
-  v->item_work = 16384;
+// The baseline's items: every matrix with the default variant for its k and
+// items small enough that one launch per matrix spreads over all SMs.
+static uint32_t grid_filling_cap(const sparsep_batch *b, uint32_t m, uint32_t cap) {
+  const uint64_t want = (b->nnz[m] + 2ull * b->sms - 1) / (2ull * b->sms);
+  return (uint32_t)std::min<uint64_t>(cap, std::max<uint64_t>(64, want));
 }
 
 template <typename T>
@@ -303,20 +236,24 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
   b->var.resize(nmats);
   b->item0.resize(nmats);
   b->nitem.resize(nmats);
-  std::vector<std::vector<uint32_t>> rowptrs(nmats);
+  b->base0.resize(nmats);
+  b->nbase.resize(nmats);
+  b->rowptr.resize(nmats);
   for (uint32_t m = 0; m < nmats; ++m) {
     const auto *M = A[m];
     if (!M || !M->rowptr || (M->nnz && (!M->colind || !M->values))) return SPARSEP_EINVAL;
     const uint32_t k = nrhs[m];
     if (k == 0 || k > 256) return SPARSEP_EINVAL;
-    if (M->rowptr[M->nrows] != M->nnz) return SPARSEP_EINVAL;
+    if (M->rowptr[0] != 0 || M->rowptr[M->nrows] != M->nnz) return SPARSEP_EINVAL;
+    for (uint32_t r = 0; r < M->nrows; ++r)
+      if (M->rowptr[r + 1] < M->rowptr[r]) return SPARSEP_EINVAL;
     for (uint32_t q = 0; q < M->nnz; ++q)
       if (M->colind[q] >= M->ncols) return SPARSEP_EINVAL;
     if (var) b->var[m] = var[m];
     else sparsep_batch_variant_default(k, &b->var[m]);
     if (int st = check_variant(b->var[m], k)) return st;
     void *d[5];
-    int st = balloc(b, ((size_t)M->nrows + 1) * 4, &d[0]);
+    int st = balloc(b, ((size_t)M->nrows + 1 + 16) * 4, &d[0]);
     if (!st) st = balloc(b, ((size_t)M->nnz + 16) * 4, &d[1]);
     if (!st) st = balloc(b, ((size_t)M->nnz + 16) * sizeof(T), &d[2]);
     if (!st) st = balloc(b, ((size_t)M->ncols * k + 16) * sizeof(T), &d[3]);
@@ -339,53 +276,47 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
     h.k = k;
     h.pad = 0;
     b->nnz[m] = M->nnz;
-    rowptrs[m].assign(M->rowptr, M->rowptr + M->nrows + 1);
+    b->rowptr[m].assign(M->rowptr, M->rowptr + M->nrows + 1);
     b->bytes += (uint64_t)M->nnz * (4 + sizeof(T)) + ((uint64_t)M->nrows + 1) * 4 +
                 ((uint64_t)M->ncols + M->nrows) * k * sizeof(T);
   }
-  for (uint32_t m = 0; m < nmats; ++m) make_items(b, m, rowptrs[m].data());
-  int st = balloc(b, sizeof(Mat<T>) * nmats, &b->mats_d);
-  if (!st) st = balloc(b, sizeof(BItem) * b->items_h.size(), (void **)&b->items_d);
+  for (uint32_t m = 0; m < nmats; ++m) {
+    sparsep_batch_variant dv;
+    sparsep_batch_variant_default(b->mats_h[m].k, &dv);
+    b->base0[m] = (uint32_t)b->base_h.size();
+    make_items(b->mats_h[m], b->rowptr[m].data(), dv, grid_filling_cap(b, m, item_cap(dv, b->mats_h[m].k)),
+               b->base_h);
+    b->nbase[m] = (uint32_t)b->base_h.size() - b->base0[m];
+  }
+  int st = balloc(b, 64, (void **)&b->err);
+  if (!st) st = balloc(b, sizeof(BItem) * std::max<size_t>(1, b->base_h.size()), (void **)&b->base_d);
   if (!st) st = balloc(b, 64, (void **)&b->head);
   if (st) return st;
-  BCK(cudaMemcpy(b->mats_d, b->mats_h.data(), sizeof(Mat<T>) * nmats, cudaMemcpyHostToDevice));
-  BCK(cudaMemcpy(b->items_d, b->items_h.data(), sizeof(BItem) * b->items_h.size(), cudaMemcpyHostToDevice));
+  BCK(cudaMemset(b->err, 0, 64));
+  if (!b->base_h.empty())
+    BCK(cudaMemcpy(b->base_d, b->base_h.data(), sizeof(BItem) * b->base_h.size(), cudaMemcpyHostToDevice));
+  if ((st = rebuild(b))) return st;
   BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  int per_sm = 0;
-  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent<T>, 256, 0));
-  b->grid = b->sms * std::max(per_sm, 1);
   *out = guard.release();
   return SPARSEP_OK;
 }
 
 template <typename T>
-static int launch_persistent(sparsep_batch *b, cudaStream_t s) {
-  BCK(cudaMemsetAsync(b->head, 0, 4, s));
-  persistent<T><<<b->grid, 256, 0, s>>>((const Mat<T> *)b->mats_d, b->items_d, (uint32_t)b->items_h.size(),
-                                         b->head);
-  return bmap(cudaGetLastError());
+static int launch_queue(sparsep_batch *b, cudaStream_t s) {
+  if (b->ticket) BCK(cudaMemsetAsync(b->head, 0, 4, s));
+  return bmap(batch_launch<T>(b->queue_d, 0, (uint32_t)b->items_h.size(), b->ticket ? b->head : nullptr, b->err, s));
 }
 
 template <typename T>
-static int launch_one(sparsep_batch *b, uint32_t m, cudaStream_t s) {
-  const uint32_t n = b->nitem[m];
-  if (!n) return SPARSEP_OK;
-  per_matrix<T><<<(n + 7) / 8, 256, 0, s>>>((const Mat<T> *)b->mats_d, b->items_d, b->item0[m], n);
-  return bmap(cudaGetLastError());
+static int launch_items(sparsep_batch *b, const BItem *items, uint32_t i0, uint32_t n, cudaStream_t s) {
+  return bmap(batch_launch<T>(items, i0, n, nullptr, b->err, s));
 }
 
-static int dispatch_persistent(sparsep_batch *b, cudaStream_t s) {
-  return b->dtype == SPARSEP_FP32 ? launch_persistent<float>(b, s) : launch_persistent<int32_t>(b, s);
+static int dispatch_queue(sparsep_batch *b, cudaStream_t s) {
+  return b->dtype == SPARSEP_FP32 ? launch_queue<float>(b, s) : launch_queue<int32_t>(b, s);
 }
-static int dispatch_one(sparsep_batch *b, uint32_t m, cudaStream_t s) {
-  return b->dtype == SPARSEP_FP32 ? launch_one<float>(b, m, s) : launch_one<int32_t>(b, m, s);
-}
-
-static void drop_graph(sparsep_batch *b) {
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->graph) cudaGraphDestroy(b->graph);
-  b->exec = nullptr;
-  b->graph = nullptr;
+static int dispatch_items(sparsep_batch *b, const BItem *items, uint32_t i0, uint32_t n, cudaStream_t s) {
+  return b->dtype == SPARSEP_FP32 ? launch_items<float>(b, items, i0, n, s) : launch_items<int32_t>(b, items, i0, n, s);
 }
 
 extern "C" {
@@ -411,7 +342,8 @@ int sparsep_batch_create_i32(uint32_t nmats, const sparsep_csr_i32 *const *A, co
 void sparsep_batch_free(sparsep_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
-  drop_graph(b);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
   for (void *d : b->allocs) cudaFree(d);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -424,30 +356,20 @@ int sparsep_batch_set_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_
   return SPARSEP_OK;
 }
 
-// Rebuild the item queue after variants changed (needs each matrix's rowptr,
-// read back from the device).
+int sparsep_batch_get_variant(const sparsep_batch *b, uint32_t m, sparsep_batch_variant *v) {
+  if (!b || !v || m >= b->nmats) return SPARSEP_EINVAL;
+  *v = b->var[m];
+  return SPARSEP_OK;
+}
+
+// Rebuild the items and the queue after variants changed.
 int sparsep_batch_commit(sparsep_batch *b) {
   if (!b) return SPARSEP_EINVAL;
-  drop_graph(b);
-  b->items_h.clear();
-  for (uint32_t m = 0; m < b->nmats; ++m) {
-    std::vector<uint32_t> rp((size_t)b->mats_h[m].nrows + 1);
-    BCK(cudaMemcpy(rp.data(), b->mats_h[m].rowptr, rp.size() * 4, cudaMemcpyDeviceToHost));
-    make_items(b, m, rp.data());
+  try {
+    return rebuild(b);
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
   }
-  // replace the device item array
-  for (auto i = b->allocs.begin(); i != b->allocs.end(); ++i)
-    if (*i == (void *)b->items_d) {
-      cudaFree(*i);
-      b->allocs.erase(i);
-      break;
-    }
-  void *d = nullptr;
-  int st = balloc(b, sizeof(BItem) * b->items_h.size(), &d);
-  if (st) return st;
-  b->items_d = (BItem *)d;
-  BCK(cudaMemcpy(b->items_d, b->items_h.data(), sizeof(BItem) * b->items_h.size(), cudaMemcpyHostToDevice));
-  return SPARSEP_OK;
 }
 
 int sparsep_batch_x(sparsep_batch *b, uint32_t m, void **d_x, void **d_y) {
@@ -471,14 +393,14 @@ int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y) {
   return SPARSEP_OK;
 }
 
-// The whole batch: one graph launch (queue reset + persistent kernel); the
+// The whole batch: one graph launch (queue reset + queue kernel); the
 // graph is captured on the first call after a (re)commit.
 int sparsep_batch_execute(sparsep_batch *b, void *stream) {
   if (!b) return SPARSEP_EINVAL;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
   if (!b->exec) {
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    int st = dispatch_persistent(b, b->stream);
+    int st = dispatch_queue(b, b->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (st) {
@@ -490,37 +412,42 @@ int sparsep_batch_execute(sparsep_batch *b, void *stream) {
     BCK(cudaGraphInstantiate(&b->exec, b->graph, 0));
   }
   BCK(cudaGraphLaunch(b->exec, s));
-  if (!stream) BCK(cudaStreamSynchronize(s));
-  return SPARSEP_OK;
+  if (stream) return SPARSEP_OK;
+  BCK(cudaStreamSynchronize(s));
+  return sparsep_batch_status(b);
 }
 
-// The baseline: one kernel launch per matrix on `stream`, in matrix order.
+// The baseline: one plain launch per matrix, in matrix order, each matrix with
+// the default (untuned) variant for its k and items sized to fill the GPU.
 int sparsep_batch_execute_per_matrix(sparsep_batch *b, void *stream) {
   if (!b) return SPARSEP_EINVAL;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
   for (uint32_t m = 0; m < b->nmats; ++m)
-    if (int st = dispatch_one(b, m, s)) return st;
-  if (!stream) BCK(cudaStreamSynchronize(s));
-  return SPARSEP_OK;
+    if (int st = dispatch_items(b, b->base_d, b->base0[m], b->nbase[m], s)) return st;
+  if (stream) return SPARSEP_OK;
+  BCK(cudaStreamSynchronize(s));
+  return sparsep_batch_status(b);
 }
 
-// One matrix alone (autotuner timing runs).
+// One matrix alone with its committed items.
 int sparsep_batch_execute_one(sparsep_batch *b, uint32_t m, void *stream) {
   if (!b || m >= b->nmats) return SPARSEP_EINVAL;
-  return dispatch_one(b, m, static_cast<cudaStream_t>(stream));
+  return dispatch_items(b, b->items_d, b->item0[m], b->nitem[m], static_cast<cudaStream_t>(stream));
 }
 
 // Exhaustive autotuner over the row-routine variants of every matrix: each
-// candidate's items are built, uploaded to a scratch item array and timed
-// alone with CUDA events (median of `reps`); the fastest is kept.  The chosen
-// variants are committed (items rebuilt, graph recaptured on next execute).
-// times_us (nmats x sparsep_batch_candidates()) receives the medians, 0 for
-// candidates that do not apply to a matrix; chosen (nmats) the chosen index.
+// candidate's items (sized to fill the GPU) are uploaded to a scratch array
+// and timed alone with CUDA events (median of `reps`, after one warm-up); the
+// fastest is kept.  The chosen variants are committed (items rebuilt, graph
+// recaptured on the next execute).  times_us (nmats x candidates) receives
+// the medians, 0 where a candidate does not apply; chosen (nmats) the index.
 static const sparsep_batch_variant kCand[] = {
-    {0, 4, 16384, 0},  {0, 8, 16384, 0},  {0, 16, 16384, 0},  {0, 32, 16384, 0}, {0, 4, 131072, 0},
-    {0, 8, 131072, 0}, {0, 16, 131072, 0}, {0, 32, 131072, 0}, {1, 1, 16384, 0},  {1, 2, 16384, 0},
-    {1, 4, 16384, 0},  {1, 8, 16384, 0},  {1, 16, 16384, 0},  {1, 32, 16384, 0}, {1, 1, 131072, 0},
-    {1, 4, 131072, 0}, {1, 8, 131072, 0}, {1, 32, 131072, 0}};
+    {0, 1, 0, 1},  {0, 1, 0, 2},  {0, 1, 0, 4},  {0, 2, 0, 1},  {0, 2, 0, 2},  {0, 2, 0, 4},
+    {0, 4, 0, 1},  {0, 4, 0, 2},  {0, 4, 0, 4},  {0, 8, 0, 1},  {0, 8, 0, 2},  {0, 8, 0, 4},
+    {0, 16, 0, 1}, {0, 16, 0, 2}, {0, 16, 0, 4}, {0, 32, 0, 1}, {0, 32, 0, 2}, {0, 32, 0, 4},
+    {1, 1, 0, 1},  {1, 1, 0, 2},  {1, 1, 0, 4},  {1, 2, 0, 1},  {1, 2, 0, 2},  {1, 2, 0, 4},
+    {1, 4, 0, 1},  {1, 4, 0, 2},  {1, 4, 0, 4},  {1, 8, 0, 1},  {1, 8, 0, 2},  {1, 8, 0, 4},
+    {1, 16, 0, 1}, {1, 16, 0, 2}, {1, 16, 0, 4}, {1, 32, 0, 1}, {1, 32, 0, 2}, {1, 32, 0, 4}};
 constexpr int kNCand = sizeof(kCand) / sizeof(kCand[0]);
 
 int sparsep_batch_candidates(sparsep_batch_variant *out, int max) {
@@ -528,72 +455,88 @@ int sparsep_batch_candidates(sparsep_batch_variant *out, int max) {
   return kNCand;
 }
 
+int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v, int reps,
+                               double *us_out);
+
 int sparsep_batch_autotune(sparsep_batch *b, int reps, double *times_us, int32_t *chosen) {
   if (!b || reps < 1) return SPARSEP_EINVAL;
-  cudaStream_t s = b->stream;
-  cudaEvent_t e0, e1;
-  BCK(cudaEventCreate(&e0));
-  BCK(cudaEventCreate(&e1));
-  int status = SPARSEP_OK;
-  BItem *scratch = nullptr;
-  size_t scratch_n = 0;
-  std::vector<float> ms(reps);
-  for (uint32_t m = 0; m < b->nmats && !status; ++m) {
-    std::vector<uint32_t> rp((size_t)b->mats_h[m].nrows + 1);
-    if ((status = bmap(cudaMemcpy(rp.data(), b->mats_h[m].rowptr, rp.size() * 4, cudaMemcpyDeviceToHost)))) break;
+  for (uint32_t m = 0; m < b->nmats; ++m) {
     double best = 1e300;
     int best_i = -1;
-    const sparsep_batch_variant keep = b->var[m];
-    for (int c = 0; c < kNCand && !status; ++c) {
-      if (times_us) times_us[(size_t)m * kNCand + c] = 0.0;
-      if (check_variant(kCand[c], b->mats_h[m].k)) continue;
-      // candidate items of matrix m alone
-      sparsep_batch tmp;
-      tmp.mats_h = {b->mats_h[m]};
-      tmp.var = {kCand[c]};
-      tmp.item0.assign(1, 0);
-      tmp.nitem.assign(1, 0);
-      make_items(&tmp, 0, rp.data());
-      for (auto &it : tmp.items_h) it.mat = m;
-      tmp.mats_h.clear();
-      const size_t n = tmp.items_h.size();
-      if (n > scratch_n) {
-        if (scratch) cudaFree(scratch);
-        scratch = nullptr;
-        if ((status = bmap(cudaMalloc(&scratch, n * sizeof(BItem))))) break;
-        scratch_n = n;
-      }
-      if ((status = bmap(cudaMemcpy(scratch, tmp.items_h.data(), n * sizeof(BItem), cudaMemcpyHostToDevice)))) break;
-      for (int r = -1; r < reps; ++r) {  // one untimed warm-up
-        cudaEventRecord(e0, s);
-        if (b->dtype == SPARSEP_FP32)
-          per_matrix<float><<<(unsigned)((n + 7) / 8), 256, 0, s>>>((const Mat<float> *)b->mats_d, scratch, 0,
-                                                                     (uint32_t)n);
-        else
-          per_matrix<int32_t><<<(unsigned)((n + 7) / 8), 256, 0, s>>>((const Mat<int32_t> *)b->mats_d, scratch, 0,
-                                                                       (uint32_t)n);
-        cudaEventRecord(e1, s);
-        if ((status = bmap(cudaEventSynchronize(e1)))) break;
-        if (r >= 0) cudaEventElapsedTime(&ms[r], e0, e1);
-      }
-      if (status) break;
-      std::vector<float> sorted = ms;
-      std::sort(sorted.begin(), sorted.end());
-      const double us = 1e3 * sorted[sorted.size() / 2];
+    for (int c = 0; c < kNCand; ++c) {
+      double us = 0.0;
+      const int st = sparsep_batch_time_variant(b, m, &kCand[c], reps, &us);
+      if (st == SPARSEP_ENOSYS) us = 0.0;
+      else if (st) return st;
       if (times_us) times_us[(size_t)m * kNCand + c] = us;
-      if (us < best) {
+      if (us > 0.0 && us < best) {
         best = us;
         best_i = c;
       }
     }
-    b->var[m] = best_i >= 0 ? kCand[best_i] : keep;
+    if (best_i >= 0) b->var[m] = kCand[best_i];
     if (chosen) chosen[m] = best_i;
   }
-  if (scratch) cudaFree(scratch);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (status) return status;
   return sparsep_batch_commit(b);
+}
+
+// Median time (us) of matrix m alone under variant v, items sized to fill the
+// GPU; ENOSYS when v does not apply to m's right-hand-side count.
+int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v, int reps,
+                               double *us_out) {
+  if (!b || !v || !us_out || m >= b->nmats || reps < 1) return SPARSEP_EINVAL;
+  if (int st = check_variant(*v, b->mats_h[m].k)) return st;
+  std::vector<BItem> items;
+  try {
+    make_items(b->mats_h[m], b->rowptr[m].data(), *v, grid_filling_cap(b, m, item_cap(*v, b->mats_h[m].k)), items);
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
+  }
+  *us_out = 0.0;
+  if (items.empty()) return SPARSEP_OK;
+  BItem *d = nullptr;
+  BCK(cudaMalloc(&d, items.size() * sizeof(BItem)));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int st = bmap(cudaMemcpy(d, items.data(), items.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+  if (!st) st = bmap(cudaEventCreate(&e0));
+  if (!st) st = bmap(cudaEventCreate(&e1));
+  std::vector<float> ms(reps);
+  for (int r = -1; r < reps && !st; ++r) {
+    cudaEventRecord(e0, b->stream);
+    st = dispatch_items(b, d, 0, (uint32_t)items.size(), b->stream);
+    cudaEventRecord(e1, b->stream);
+    if (!st) st = bmap(cudaEventSynchronize(e1));
+    if (!st && r >= 0) st = bmap(cudaEventElapsedTime(&ms[r], e0, e1));
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(d);
+  if (st) return st;
+  std::sort(ms.begin(), ms.end());
+  *us_out = 1e3 * ms[ms.size() / 2];
+  return SPARSEP_OK;
+}
+
+// Staging timeouts since the last call (the failed items were skipped):
+// SPARSEP_ETIMEDOUT, else OK.  Synchronises the batch's work.
+int sparsep_batch_status(sparsep_batch *b) {
+  if (!b) return SPARSEP_EINVAL;
+  int h = 0;
+  BCK(cudaMemcpy(&h, b->err, sizeof h, cudaMemcpyDeviceToHost));
+  if (h) BCK(cudaMemset(b->err, 0, sizeof h));
+  return h ? SPARSEP_ETIMEDOUT : SPARSEP_OK;
+}
+
+// 1: CTAs of the batch launch claim items by atomic ticket (queue order
+// guaranteed); 0: CTA b runs queue item b (order as the hardware schedules).
+int sparsep_batch_set_ticket(sparsep_batch *b, int on) {
+  if (!b) return SPARSEP_EINVAL;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->ticket = on != 0;
+  return SPARSEP_OK;
 }
 
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz) {

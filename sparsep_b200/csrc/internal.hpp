@@ -122,4 +122,7 @@ SPARSEP_FREE_ANY(f64)
 void greedy_split(const uint64_t *prefix, uint32_t n, uint32_t parts, uint32_t *split);
 void greedy_split_bcsr(const uint64_t *prefix, uint32_t n, uint32_t parts, uint32_t *split);
 
+// Text of the last failure, returned by sparsep_last_error() on this thread.
+void record_error(const char *msg);
+
 }  // namespace sparsep

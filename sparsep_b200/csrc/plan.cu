@@ -61,6 +61,10 @@ struct sparsep_plan {
 
 static thread_local char g_last_error[256] = "";
 
+namespace sparsep {
+void record_error(const char *msg) { std::snprintf(g_last_error, sizeof g_last_error, "%s", msg); }
+}  // namespace sparsep
+
 static int map_cuda(cudaError_t e) {
   if (e != cudaSuccess) std::snprintf(g_last_error, sizeof g_last_error, "%s (%d)", cudaGetErrorString(e), (int)e);
   switch (e) {

@@ -70,7 +70,7 @@ def test_batch_every_candidate(dtype):
         applied = False
         for m, d in enumerate(data):
             k = d[4]
-            if (v.mode == 0 and 4 <= k <= 8 * v.lanes) or (v.mode == 1 and k <= 4):
+            if v.applies(k):
                 b.set_variant(m, v)
                 applied = True
         if not applied:
