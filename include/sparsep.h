@@ -489,7 +489,7 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
 /* ------------------------------------------------------------------------ */
 /* Many CSR matrices, each with its own k = 1..256 right-hand sides (x is
  * ncols x k and y nrows x k, row-major), multiplied by ONE kernel launch:
- * its CTAs claim work items (row ranges of any matrix, at most 2048 nonzeros,
+ * its CTAs claim work items (row ranges of any matrix, at most 4096 nonzeros,
  * or one longer row) from a device work queue by atomic ticket, replayed as a
  * CUDA graph (queue reset + kernel).  The row routine of each matrix is a
  * variant: the CTA is cut into groups of `lanes` (1..32, power of two) lanes,
@@ -498,7 +498,7 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
  *   mode 0: the rows of a work item dealt round-robin to the groups;
  *   mode 1: the rows and nonzeros of a work item split evenly over the groups
  *           (merge path), rows cut by a split finished from carries;
- *   item_work: nonzero x right-hand-side products per item (0 = 16384).
+ *   item_work: nonzero x right-hand-side products per item (0 = 65536).
  * FP32 and INT32 (integers wrap exactly, as the single-vector path).  Status
  * ENOSYS: the variant does not apply to that k. */
 typedef struct sparsep_batch sparsep_batch;

@@ -82,7 +82,7 @@ static uint32_t pow2ceil(uint32_t v) {
   return p;
 }
 
-static constexpr uint32_t DEFAULT_ITEM_WORK = 16384;  // nonzero x right-hand-side products per item
+static constexpr uint32_t DEFAULT_ITEM_WORK = 65536;  // nonzero x right-hand-side products per item
 
 // Nonzeros per item for a variant: about item_work products, within [32, BCAP].
 static uint32_t item_cap(const sparsep_batch_variant &v, uint32_t k) {
@@ -105,7 +105,8 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparse
   base.val = M.val;
   base.x = M.x;
   base.y = M.y;
-  base.k = k;
+  base.k = (uint16_t)k;
+  base.ncols = M.ncols;
   BItem cur{};
   bool open = false;
   auto flush = [&]() {
@@ -118,7 +119,7 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparse
       flush();
       BItem it = base;
       it.r0 = r;
-      it.r1 = r + 1;
+      it.nr = 1;
       it.p0 = rowptr[r];
       it.p1 = rowptr[r + 1];
       it.mode = MODE_LONG;
@@ -128,10 +129,11 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparse
       out.push_back(it);
       continue;
     }
-    if (open && (cur.p1 - cur.p0 + len > cap || cur.r1 - cur.r0 == BRCAP)) flush();
+    if (open && (cur.p1 - cur.p0 + len > cap || cur.nr == BRCAP)) flush();
     if (!open) {
       cur = base;
-      cur.r0 = cur.r1 = r;
+      cur.r0 = r;
+      cur.nr = 0;
       cur.p0 = cur.p1 = rowptr[r];
       cur.mode = v.mode == 0 ? MODE_ROWS : MODE_MERGE;
       cur.lanes = (uint8_t)v.lanes;
@@ -139,7 +141,7 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparse
       cur.acc = (uint8_t)acc;
       open = true;
     }
-    cur.r1 = r + 1;
+    cur.nr = (uint16_t)(r + 1 - cur.r0);
     cur.p1 = rowptr[r + 1];
   }
   flush();
@@ -523,8 +525,13 @@ int sparsep_batch_status(sparsep_batch *b) {
   if (!b) return SPARSEP_EINVAL;
   int h = 0;
   BCK(cudaMemcpy(&h, b->err, sizeof h, cudaMemcpyDeviceToHost));
-  if (h) BCK(cudaMemset(b->err, 0, sizeof h));
-  return h ? SPARSEP_ETIMEDOUT : SPARSEP_OK;
+  if (!h) return SPARSEP_OK;
+  BCK(cudaMemset(b->err, 0, sizeof h));
+  if (h == SPARSEP_ETIMEDOUT) return h;
+  char msg[96];
+  std::snprintf(msg, sizeof msg, "batch kernel check failed at site %d", h);  // checked build only
+  sparsep::record_error(msg);
+  return SPARSEP_EIO;
 }
 
 // 1: CTAs of the batch launch claim items by atomic ticket (queue order

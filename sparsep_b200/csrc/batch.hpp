@@ -19,8 +19,8 @@ template <typename T> struct Mat {
 };
 
 constexpr int BT = 256;            // threads per CTA
-constexpr uint32_t BCAP = 2048;    // nonzeros staged per item (and per long-row chunk)
-constexpr uint32_t BRCAP = 512;    // rows per item
+constexpr uint32_t BCAP = 4096;    // nonzeros staged per item (and per long-row chunk)
+constexpr uint32_t BRCAP = 1024;   // rows per item
 constexpr int ACC_REGS = 8;        // V * ACC accumulators per lane
 
 enum : uint8_t { MODE_ROWS = 0, MODE_MERGE = 1, MODE_LONG = 2 };
@@ -32,9 +32,11 @@ struct BItem {
   const void *val;
   const void *x;
   void *y;
-  uint32_t k;       // right-hand sides (x: ncols x k, y: nrows x k, row-major)
-  uint32_t r0, r1;  // rows [r0, r1)
-  uint32_t p0, p1;  // nonzeros [p0, p1) = rowptr[r0] .. rowptr[r1]
+  uint32_t r0;      // rows [r0, r0 + nr)
+  uint32_t p0, p1;  // nonzeros [p0, p1) = rowptr[r0] .. rowptr[r0 + nr]
+  uint32_t ncols;   // columns of the matrix (bounds of x)
+  uint16_t nr;      // rows (<= BRCAP)
+  uint16_t k;       // right-hand sides (x: ncols x k, y: nrows x k, row-major)
   uint8_t mode, lanes, vec, acc;
 };
 static_assert(sizeof(BItem) == 64, "item layout");

@@ -47,6 +47,7 @@ template <typename T> struct View {
   const T *x;
   T *y;
   uint32_t k;
+  uint32_t ncols;
 };
 
 // The staged arrays, indexed from the item's first row / nonzero.
@@ -54,7 +55,19 @@ template <typename T> struct Staged {
   const uint32_t *rp;  // rp[i] = rowptr[r0 + i]
   const uint32_t *col; // col[q] = colind[p0 + q]
   const T *val;
+  uint32_t n;          // staged nonzeros
+  int *err;
 };
+
+// Index guards: a failed check records its site code in the error word
+// (read by sparsep_batch_status) and the guarded access is skipped, so a
+// corrupted item or column index cannot take the GPU down.  The cheap ones
+// (per item, per gathered column) are always on; the checked build
+// (-DSPARSEP_CHECK) adds a full scan of each staged rowptr slice.
+__device__ __forceinline__ bool bchk(bool ok, int *err, int code) {
+  if (!ok && err) atomicCAS(err, 0, code);
+  return ok;
+}
 
 template <typename T, int V> struct VecT;
 template <typename T> struct VecT<T, 1> {
@@ -189,11 +202,18 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &
                                           uint32_t e, int gl) {
   constexpr int U = 16 / (V * ACC) > 2 ? 16 / (V * ACC) : 2;
   const uint32_t k = m.k;
+  if (!bchk(q <= e && e <= s.n, s.err, -2101)) return;
+  // columns are clamped into x (in bounds whatever the staged data); a clamp
+  // that changed a column is recorded once for the range
+  const uint32_t cmax = m.ncols - 1;
+  uint32_t bad = 0;
   for (; q + U <= e; q += U) {
     uint32_t c[U];
     T v[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) c[u] = s.col[q + u], v[u] = s.val[q + u];
+#pragma unroll
+    for (int u = 0; u < U; ++u) bad |= c[u] > cmax, c[u] = min(c[u], cmax);
     VecT<T, V> xv[U][ACC];
 #pragma unroll
     for (int a = 0; a < ACC; ++a) {
@@ -213,7 +233,9 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &
     }
   }
   for (; q < e; ++q) {
-    const T *xr = m.x + (size_t)s.col[q] * k;
+    const uint32_t cq = min(s.col[q], cmax);
+    bad |= s.col[q] > cmax;
+    const T *xr = m.x + (size_t)cq * k;
     const T v = s.val[q];
 #pragma unroll
     for (int a = 0; a < ACC; ++a) {
@@ -225,6 +247,7 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &
       }
     }
   }
+  bchk(!bad, s.err, -2106);
 }
 
 template <typename T, int G, int V, int ACC>
@@ -244,7 +267,7 @@ __device__ __forceinline__ void item_rows(const View<T> &m, const Staged<T> &s, 
   using A = Acc<T>;
   constexpr int NG = BT / G;
   const int gi = tid / G, gl = tid % G;
-  const uint32_t nr = it.r1 - it.r0;
+  const uint32_t nr = it.nr;
   for (uint32_t lr = gi; lr < nr; lr += NG) {
     A acc[ACC][V];
     zero_acc<T, V, ACC>(acc);
@@ -279,11 +302,12 @@ __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s,
   using A = Acc<T>;
   constexpr int NG = BT / G;
   const int gi = tid / G, gl = tid % G;
-  const uint32_t k = m.k, nr = it.r1 - it.r0, n = it.p1 - it.p0, total = nr + n;
+  const uint32_t k = m.k, nr = it.nr, n = it.p1 - it.p0, total = nr + n;
   const uint32_t d0 = (uint32_t)((uint64_t)total * gi / NG), d1 = (uint32_t)((uint64_t)total * (gi + 1) / NG);
   const uint32_t i0 = merge_search(s.rp, it.p0, nr, n, d0), i1 = merge_search(s.rp, it.p0, nr, n, d1);
   const uint32_t j1 = d1 - i1;
   uint32_t j = d0 - i0;
+  bchk(i0 <= i1 && i1 <= nr && j <= j1 && j1 <= n, s.err, -2102);
   A head[ACC][V], acc[ACC][V];
   zero_acc<T, V, ACC>(head);
   for (uint32_t r = i0; r < i1; ++r) {
@@ -344,16 +368,19 @@ __device__ __forceinline__ void item_long(const View<T> &m, const BItem &it, BSh
   const uint32_t k = m.k;
   A acc[ACC][1];
   zero_acc<T, 1, ACC>(acc);
-  uint32_t parity = 0;
+  uint32_t parity = 0, bad = 0;
   for (uint32_t c0 = it.p0; c0 < it.p1; c0 += BCAP, parity ^= 1u) {
     const uint32_t n = min(BCAP, it.p1 - c0);
     const Window wc = window(it.colind, c0, c0 + n, 4), wv = window(it.val, c0, c0 + n, sizeof(T));
+    if (!bchk(wc.bytes <= sizeof(sh.col) && wv.bytes <= sizeof(sh.val), err, -2103)) return;
     __syncthreads();  // the previous chunk is consumed
     if (tid == 0) issue(&sh.bar, sh.col, wc, sh.val, wv, nullptr, Window{0, 0, 0});
     if (!landed(&sh.bar, parity, err)) return;
-    const Staged<T> s{nullptr, sh.col + wc.lead, sh.val + wv.lead};
+    const Staged<T> s{nullptr, sh.col + wc.lead, sh.val + wv.lead, n, err};
     for (uint32_t q = gi; q < n; q += NG) {
-      const T *xr = m.x + (size_t)s.col[q] * k;
+      const uint32_t cq = min(s.col[q], m.ncols - 1);
+      bad |= s.col[q] >= m.ncols;
+      const T *xr = m.x + (size_t)cq * k;
       const T v = s.val[q];
 #pragma unroll
       for (int a = 0; a < ACC; ++a) {
@@ -362,6 +389,7 @@ __device__ __forceinline__ void item_long(const View<T> &m, const BItem &it, BSh
       }
     }
   }
+  bchk(!bad, err, -2107);
   __syncthreads();
   A *red = reinterpret_cast<A *>(sh.col);
 #pragma unroll
@@ -450,7 +478,7 @@ __global__ void __launch_bounds__(BT) batch_items(const BItem *items, uint32_t i
   }
   __syncthreads();
   const BItem it = items[head ? sh.next : i0 + blockIdx.x];
-  const View<T> m{static_cast<const T *>(it.x), static_cast<T *>(it.y), it.k};
+  const View<T> m{static_cast<const T *>(it.x), static_cast<T *>(it.y), it.k, it.ncols};
   if (it.mode == MODE_LONG) {
     switch (it.lanes) {
       case 1: long_acc<T, 1>(m, it, sh, tid, err); break;
@@ -462,12 +490,24 @@ __global__ void __launch_bounds__(BT) batch_items(const BItem *items, uint32_t i
     }
     return;
   }
-  const Window wr = window(it.rowptr, it.r0, it.r1 + 1, 4);
+  const Window wr = window(it.rowptr, it.r0, it.r0 + it.nr + 1, 4);
   const Window wc = window(it.colind, it.p0, it.p1, 4);
   const Window wv = window(it.val, it.p0, it.p1, sizeof(T));
+  if (!bchk(wr.bytes <= sizeof(sh.rp) && wc.bytes <= sizeof(sh.col) && wv.bytes <= sizeof(sh.val) &&
+                it.nr <= BRCAP && it.p1 - it.p0 <= BCAP,
+            err, -2104))
+    return;
   if (tid == 0) issue(&sh.bar, sh.rp, wr, sh.col, wc, sh.val, wv);
   if (!landed(&sh.bar, 0, err)) return;
-  const Staged<T> s{sh.rp + wr.lead, sh.col + wc.lead, sh.val + wv.lead};
+  const Staged<T> s{sh.rp + wr.lead, sh.col + wc.lead, sh.val + wv.lead, it.p1 - it.p0, err};
+  {
+    // the staged rowptr must run from p0 to p1 (checked build: non-decreasing)
+    bool ok = s.rp[0] == it.p0 && s.rp[it.nr] == it.p1;
+#ifdef SPARSEP_CHECK
+    for (uint32_t i = tid; i < it.nr; i += BT) ok = ok && s.rp[i] <= s.rp[i + 1];
+#endif
+    if (__syncthreads_or(!bchk(ok, err, -2105))) return;
+  }
   if (it.mode == MODE_ROWS) by_lanes<T, MODE_ROWS>(m, s, it, sh, tid);
   else by_lanes<T, MODE_MERGE>(m, s, it, sh, tid);
 }
