@@ -546,6 +546,49 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
 
 /* ------------------------------------------------------------------------ */
+/* Learned variant selector (no reference counterpart)                       */
+/* ------------------------------------------------------------------------ */
+/* Sixteen cheap sparsity features of a CSR structure with k right-hand sides
+ * (log sizes, row-length mean / spread / max, long- and short-row shares,
+ * distance from the diagonal, 4x4 and 8x8 block fill, x footprint, column
+ * step), an MLP 16-64-64-K over them (BF16 weights, FP32 accumulate; K =
+ * SPARSEP_NVARIANTS = the batch variants of sparsep_batch_candidates, in that
+ * order), and its hand-written CUDA training and inference kernels.  The
+ * selector only chooses a batch variant; results are those of the variant. */
+#define SPARSEP_NFEATURES 16
+#define SPARSEP_NVARIANTS 36
+int sparsep_features(uint32_t nrows, uint32_t ncols, const uint32_t *rowptr, const uint32_t *colind, uint32_t k,
+                     float *out);
+/* network primitives on device buffers: weights d_wb (BF16 bits, nparams),
+ * standardised features d_x (n x 16), times d_t (n x K, 0 = variant does not
+ * apply); loss_grad writes the mean expected-regret loss and its gradient
+ * (d_scratch: sparsep_mlp_scratch_floats(n) floats); adam updates the FP32
+ * master weights and their BF16 copy */
+uint32_t sparsep_mlp_nparams(void);
+size_t sparsep_mlp_scratch_floats(uint32_t n);
+int sparsep_mlp_forward(const uint16_t *d_wb, const float *d_x, uint32_t n, float *d_logits, void *stream);
+int sparsep_mlp_loss_grad(const uint16_t *d_wb, const float *d_x, const float *d_t, uint32_t n, float wscale,
+                          float *d_grad, float *d_loss, float *d_scratch, void *stream);
+int sparsep_mlp_adam(float *d_w, uint16_t *d_wb, const float *d_grad, float *d_m, float *d_v, uint32_t step,
+                     float lr, float beta1, float beta2, float eps, float weight_decay, void *stream);
+int sparsep_mlp_to_bf16(const float *d_w, uint16_t *d_wb, void *stream);
+/* a trained network (host BF16 weights, feature standardisation) on the GPU */
+typedef struct sparsep_selector sparsep_selector;
+int sparsep_selector_create(const uint16_t *wb, const float *feat_mean, const float *feat_std,
+                            sparsep_selector **out);
+void sparsep_selector_free(sparsep_selector *s);
+int sparsep_selector_scores(sparsep_selector *s, const float *feats, uint32_t n, float *logits);
+/* features of every matrix of a batch (nmats x 16, computed at creation) */
+int sparsep_batch_features(const sparsep_batch *b, float *out);
+/* learned variants for the whole batch: each matrix gets the applicable
+ * variant the network scores highest; where that variant's softmax
+ * probability is below min_confidence, the matrix is autotuned exhaustively
+ * instead (reps timings per candidate).  Commits.  chosen / fallback (nmats,
+ * may be NULL) receive the candidate index and 1 where the fallback ran. */
+int sparsep_batch_select(sparsep_batch *b, sparsep_selector *s, float min_confidence, int reps, int32_t *chosen,
+                         int32_t *fallback);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free SpMV                                                      */
 /* ------------------------------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device

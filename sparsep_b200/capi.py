@@ -428,6 +428,22 @@ def _batch_sigs(L):
     L.sparsep_batch_get_info.argtypes = [PB, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.sparsep_batch_variant_default.argtypes = [C.c_uint32, C.POINTER(BatchVariant)]
     L.sparsep_batch_variant_default.restype = None
+    L.sparsep_batch_features.argtypes = [PB, C.c_void_p]
+    L.sparsep_batch_select.argtypes = [PB, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+    L.sparsep_features.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+    L.sparsep_mlp_nparams.restype = C.c_uint32
+    L.sparsep_mlp_scratch_floats.argtypes = [C.c_uint32]
+    L.sparsep_mlp_scratch_floats.restype = C.c_size_t
+    L.sparsep_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+    L.sparsep_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sparsep_mlp_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                   C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
+    L.sparsep_mlp_to_bf16.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sparsep_selector_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.sparsep_selector_free.argtypes = [C.c_void_p]
+    L.sparsep_selector_free.restype = None
+    L.sparsep_selector_scores.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     L._batch_sigs = True
 
 
@@ -507,6 +523,20 @@ class Batch:
     def commit(self):
         check(lib().sparsep_batch_commit(self.h), "batch_commit")
 
+    def features(self) -> np.ndarray:
+        out = np.zeros((len(self.mats), NFEATURES), dtype=np.float32)
+        check(lib().sparsep_batch_features(self.h, out.ctypes.data), "batch_features")
+        return out
+
+    def select(self, selector: "Selector", min_confidence: float = 0.0, reps: int = 3):
+        """Learned variants (exhaustive autotuning where the network's
+        confidence is below min_confidence); returns (chosen, fallback)."""
+        ch = np.zeros(len(self.mats), dtype=np.int32)
+        fb = np.zeros(len(self.mats), dtype=np.int32)
+        check(lib().sparsep_batch_select(self.h, selector.h, float(min_confidence), int(reps), ch.ctypes.data,
+                                         fb.ctypes.data), "batch_select")
+        return ch, fb
+
     def autotune(self, reps: int = 3):
         nc = lib().sparsep_batch_candidates(None, 0)
         t = np.zeros((len(self.mats), nc), dtype=np.float64)
@@ -523,6 +553,59 @@ class Batch:
     def free(self):
         if getattr(self, "h", None) and self.h.value:
             lib().sparsep_batch_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# learned variant selector
+# ---------------------------------------------------------------------------
+NFEATURES = 16
+NVARIANTS = 36
+
+
+def features(nrows: int, ncols: int, rowptr: np.ndarray, colind: np.ndarray, k: int) -> np.ndarray:
+    """The selector's 16 features of a CSR structure with k right-hand sides."""
+    L = lib()
+    _batch_sigs(L)
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    colind = np.ascontiguousarray(colind, dtype=np.uint32)
+    out = np.zeros(NFEATURES, dtype=np.float32)
+    check(L.sparsep_features(nrows, ncols, rowptr.ctypes.data, colind.ctypes.data, int(k), out.ctypes.data),
+          "features")
+    return out
+
+
+class Selector:
+    """A trained network (BF16 weight bits + feature standardisation) on the GPU."""
+
+    def __init__(self, wb: np.ndarray, mean: np.ndarray, std: np.ndarray):
+        L = lib()
+        _batch_sigs(L)
+        self.wb = np.ascontiguousarray(wb, dtype=np.uint16)
+        self.mean = np.ascontiguousarray(mean, dtype=np.float32)
+        self.std = np.ascontiguousarray(std, dtype=np.float32)
+        assert self.wb.size == L.sparsep_mlp_nparams() and self.mean.size == NFEATURES == self.std.size
+        h = C.c_void_p()
+        check(L.sparsep_selector_create(self.wb.ctypes.data, self.mean.ctypes.data, self.std.ctypes.data,
+                                        C.byref(h)), "selector_create")
+        self.h = h
+
+    def scores(self, feats: np.ndarray) -> np.ndarray:
+        feats = np.ascontiguousarray(feats, dtype=np.float32).reshape(-1, NFEATURES)
+        out = np.zeros((feats.shape[0], NVARIANTS), dtype=np.float32)
+        check(lib().sparsep_selector_scores(self.h, feats.ctypes.data, feats.shape[0], out.ctypes.data),
+              "selector_scores")
+        return out
+
+    def free(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().sparsep_selector_free(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

@@ -3,11 +3,13 @@
 // launch, the per-matrix baseline and the exhaustive variant autotuner.  The
 // kernels are in batch_kernels.cu.
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "batch.hpp"
@@ -25,6 +27,7 @@ struct sparsep_batch {
   std::vector<Mat<float>> mats_h;  // pointers are type-agnostic; values reinterpreted per dtype
   std::vector<uint64_t> nnz;
   std::vector<std::vector<uint32_t>> rowptr;  // host copies: items are rebuilt without a read-back
+  std::vector<float> feat;                    // nmats x SPARSEP_NFEATURES selector features
   std::vector<sparsep_batch_variant> var;
   std::vector<BItem> items_h;          // committed items, matrix after matrix
   std::vector<uint32_t> item0, nitem;  // per matrix: first item and count
@@ -206,9 +209,12 @@ static int rebuild(sparsep_batch *b) {
   if (!st) st = balloc(b, bytes, (void **)&b->queue_d);
   if (st) return st;
   if (!b->items_h.empty()) {
-    BCK(cudaMemcpy(b->items_d, b->items_h.data(), sizeof(BItem) * b->items_h.size(), cudaMemcpyHostToDevice));
-    BCK(cudaMemcpy(b->queue_d, q.data(), sizeof(BItem) * q.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpyAsync(b->items_d, b->items_h.data(), sizeof(BItem) * b->items_h.size(), cudaMemcpyHostToDevice,
+                        b->stream));
+    BCK(cudaMemcpyAsync(b->queue_d, q.data(), sizeof(BItem) * q.size(), cudaMemcpyHostToDevice, b->stream));
   }
+  // landed before any launch on any stream reads them (q dies on return)
+  BCK(cudaStreamSynchronize(b->stream));
   return SPARSEP_OK;
 }
 
@@ -233,6 +239,9 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
   int dev = 0;
   BCK(cudaGetDevice(&dev));
   BCK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev));
+  // uploads and clears go on the batch's own stream, which rebuild() drains
+  // before returning: a launch on any stream then sees them complete
+  BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   b->mats_h.resize(nmats);
   b->nnz.resize(nmats);
   b->var.resize(nmats);
@@ -261,12 +270,12 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
     if (!st) st = balloc(b, ((size_t)M->ncols * k + 16) * sizeof(T), &d[3]);
     if (!st) st = balloc(b, ((size_t)M->nrows * k + 16) * sizeof(T), &d[4]);
     if (st) return st;
-    BCK(cudaMemcpy(d[0], M->rowptr, ((size_t)M->nrows + 1) * 4, cudaMemcpyHostToDevice));
+    BCK(cudaMemcpyAsync(d[0], M->rowptr, ((size_t)M->nrows + 1) * 4, cudaMemcpyHostToDevice, b->stream));
     if (M->nnz) {
-      BCK(cudaMemcpy(d[1], M->colind, (size_t)M->nnz * 4, cudaMemcpyHostToDevice));
-      BCK(cudaMemcpy(d[2], M->values, (size_t)M->nnz * sizeof(T), cudaMemcpyHostToDevice));
+      BCK(cudaMemcpyAsync(d[1], M->colind, (size_t)M->nnz * 4, cudaMemcpyHostToDevice, b->stream));
+      BCK(cudaMemcpyAsync(d[2], M->values, (size_t)M->nnz * sizeof(T), cudaMemcpyHostToDevice, b->stream));
     }
-    BCK(cudaMemset(d[3], 0, ((size_t)M->ncols * k + 16) * sizeof(T)));
+    BCK(cudaMemsetAsync(d[3], 0, ((size_t)M->ncols * k + 16) * sizeof(T), b->stream));
     auto &h = b->mats_h[m];
     h.rowptr = (const uint32_t *)d[0];
     h.colind = (const uint32_t *)d[1];
@@ -282,6 +291,19 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
     b->bytes += (uint64_t)M->nnz * (4 + sizeof(T)) + ((uint64_t)M->nrows + 1) * 4 +
                 ((uint64_t)M->ncols + M->nrows) * k * sizeof(T);
   }
+  // selector features, matrices spread over the host's threads
+  b->feat.assign((size_t)nmats * SPARSEP_NFEATURES, 0.f);
+  {
+    const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+      pool.emplace_back([&, t]() {
+        for (uint32_t m = t; m < nmats; m += nt)
+          sparsep_features(A[m]->nrows, A[m]->ncols, A[m]->rowptr, A[m]->colind, nrhs[m],
+                           &b->feat[(size_t)m * SPARSEP_NFEATURES]);
+      });
+    for (auto &th : pool) th.join();
+  }
   for (uint32_t m = 0; m < nmats; ++m) {
     sparsep_batch_variant dv;
     sparsep_batch_variant_default(b->mats_h[m].k, &dv);
@@ -294,11 +316,11 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
   if (!st) st = balloc(b, sizeof(BItem) * std::max<size_t>(1, b->base_h.size()), (void **)&b->base_d);
   if (!st) st = balloc(b, 64, (void **)&b->head);
   if (st) return st;
-  BCK(cudaMemset(b->err, 0, 64));
+  BCK(cudaMemsetAsync(b->err, 0, 64, b->stream));
   if (!b->base_h.empty())
-    BCK(cudaMemcpy(b->base_d, b->base_h.data(), sizeof(BItem) * b->base_h.size(), cudaMemcpyHostToDevice));
-  if ((st = rebuild(b))) return st;
-  BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BCK(cudaMemcpyAsync(b->base_d, b->base_h.data(), sizeof(BItem) * b->base_h.size(), cudaMemcpyHostToDevice,
+                        b->stream));
+  if ((st = rebuild(b))) return st;  // also waits for every upload above
   *out = guard.release();
   return SPARSEP_OK;
 }
@@ -384,14 +406,17 @@ int sparsep_batch_x(sparsep_batch *b, uint32_t m, void **d_x, void **d_y) {
 int sparsep_batch_set_x(sparsep_batch *b, uint32_t m, const void *h_x) {
   if (!b || !h_x || m >= b->nmats) return SPARSEP_EINVAL;
   const auto &M = b->mats_h[m];
-  BCK(cudaMemcpy((void *)M.x, h_x, (size_t)M.ncols * M.k * b->esize, cudaMemcpyHostToDevice));
+  BCK(cudaMemcpyAsync((void *)M.x, h_x, (size_t)M.ncols * M.k * b->esize, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));  // in place before any later launch, on any stream
   return SPARSEP_OK;
 }
 
 int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y) {
   if (!b || !h_y || m >= b->nmats) return SPARSEP_EINVAL;
   const auto &M = b->mats_h[m];
-  BCK(cudaMemcpy(h_y, M.y, (size_t)M.nrows * M.k * b->esize, cudaMemcpyDeviceToHost));
+  BCK(cudaStreamSynchronize(b->stream));
+  BCK(cudaMemcpyAsync(h_y, M.y, (size_t)M.nrows * M.k * b->esize, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
   return SPARSEP_OK;
 }
 
@@ -451,6 +476,7 @@ static const sparsep_batch_variant kCand[] = {
     {1, 4, 0, 1},  {1, 4, 0, 2},  {1, 4, 0, 4},  {1, 8, 0, 1},  {1, 8, 0, 2},  {1, 8, 0, 4},
     {1, 16, 0, 1}, {1, 16, 0, 2}, {1, 16, 0, 4}, {1, 32, 0, 1}, {1, 32, 0, 2}, {1, 32, 0, 4}};
 constexpr int kNCand = sizeof(kCand) / sizeof(kCand[0]);
+static_assert(kNCand == SPARSEP_NVARIANTS, "the selector scores every candidate");
 
 int sparsep_batch_candidates(sparsep_batch_variant *out, int max) {
   for (int i = 0; i < kNCand && out && i < max; ++i) out[i] = kCand[i];
@@ -499,7 +525,8 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
   BItem *d = nullptr;
   BCK(cudaMalloc(&d, items.size() * sizeof(BItem)));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  int st = bmap(cudaMemcpy(d, items.data(), items.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+  // same stream as the timed launches: the items are in place before the first
+  int st = bmap(cudaMemcpyAsync(d, items.data(), items.size() * sizeof(BItem), cudaMemcpyHostToDevice, b->stream));
   if (!st) st = bmap(cudaEventCreate(&e0));
   if (!st) st = bmap(cudaEventCreate(&e1));
   std::vector<float> ms(reps);
@@ -524,9 +551,12 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
 int sparsep_batch_status(sparsep_batch *b) {
   if (!b) return SPARSEP_EINVAL;
   int h = 0;
-  BCK(cudaMemcpy(&h, b->err, sizeof h, cudaMemcpyDeviceToHost));
+  BCK(cudaStreamSynchronize(b->stream));
+  BCK(cudaMemcpyAsync(&h, b->err, sizeof h, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
   if (!h) return SPARSEP_OK;
-  BCK(cudaMemset(b->err, 0, sizeof h));
+  BCK(cudaMemsetAsync(b->err, 0, sizeof h, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
   if (h == SPARSEP_ETIMEDOUT) return h;
   char msg[96];
   std::snprintf(msg, sizeof msg, "batch kernel check failed at site %d", h);  // checked build only
@@ -544,6 +574,55 @@ int sparsep_batch_set_ticket(sparsep_batch *b, int on) {
   b->graph = nullptr;
   b->ticket = on != 0;
   return SPARSEP_OK;
+}
+
+int sparsep_batch_features(const sparsep_batch *b, float *out) {
+  if (!b || !out) return SPARSEP_EINVAL;
+  std::memcpy(out, b->feat.data(), sizeof(float) * b->feat.size());
+  return SPARSEP_OK;
+}
+
+// Learned variants: the network's highest-scoring applicable candidate per
+// matrix; below min_confidence (softmax probability over the applicable
+// candidates) the matrix is autotuned exhaustively instead.
+int sparsep_batch_select(sparsep_batch *b, sparsep_selector *sel, float min_confidence, int reps, int32_t *chosen,
+                         int32_t *fallback) {
+  if (!b || !sel || reps < 1) return SPARSEP_EINVAL;
+  std::vector<float> z;
+  try {
+    z.resize((size_t)b->nmats * kNCand);
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
+  }
+  if (int st = sparsep_selector_scores(sel, b->feat.data(), b->nmats, z.data())) return st;
+  for (uint32_t m = 0; m < b->nmats; ++m) {
+    const float *zm = &z[(size_t)m * kNCand];
+    const uint32_t k = b->mats_h[m].k;
+    int best = -1;
+    float zmax = -3.0e38f;
+    for (int c = 0; c < kNCand; ++c)
+      if (!check_variant(kCand[c], k) && zm[c] > zmax) zmax = zm[c], best = c;
+    double sum = 0.0;
+    for (int c = 0; c < kNCand; ++c)
+      if (!check_variant(kCand[c], k)) sum += std::exp((double)zm[c] - zmax);
+    const double conf = best >= 0 ? 1.0 / sum : 0.0;
+    int fb = 0;
+    if (best < 0 || conf < min_confidence) {
+      fb = 1;
+      double tbest = 1e300;
+      for (int c = 0; c < kNCand; ++c) {
+        double us = 0.0;
+        const int st = sparsep_batch_time_variant(b, m, &kCand[c], reps, &us);
+        if (st == SPARSEP_ENOSYS) continue;
+        if (st) return st;
+        if (us > 0.0 && us < tbest) tbest = us, best = c;
+      }
+    }
+    if (best >= 0) b->var[m] = kCand[best];
+    if (chosen) chosen[m] = best;
+    if (fallback) fallback[m] = fb;
+  }
+  return sparsep_batch_commit(b);
 }
 
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz) {

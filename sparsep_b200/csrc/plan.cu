@@ -93,7 +93,9 @@ static int dalloc(sparsep_plan *p, size_t bytes, void **out) {
   if (bytes == 0) bytes = 16;
   CK(cudaMalloc(&d, bytes));
   p->allocs.push_back(d);
-  cudaError_t e = cudaMemset(d, 0, bytes);
+  // on the plan's stream: finish_plan waits for it, so every later launch,
+  // on any stream, sees the buffer complete
+  cudaError_t e = cudaMemsetAsync(d, 0, bytes, p->stream);
   if (e != cudaSuccess) return map_cuda(e);
   *out = d;
   return SPARSEP_OK;
@@ -104,7 +106,7 @@ static int upload(sparsep_plan *p, const void *h, size_t n, size_t es, size_t pa
   void *d = nullptr;
   int st = dalloc(p, (n + pad) * es, &d);
   if (st) return st;
-  if (n && h) CK(cudaMemcpy(d, h, n * es, cudaMemcpyHostToDevice));
+  if (n && h) CK(cudaMemcpyAsync(d, h, n * es, cudaMemcpyHostToDevice, p->stream));
   p->info.device_bytes += (n + pad) * es;
   *out = d;
   return SPARSEP_OK;
@@ -318,7 +320,6 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   p->smem = smem;
   int workers = o.nr_workers > 0 ? o.nr_workers : 8;
   p->threads = 32 * workers;
-  CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   for (auto &e : p->ev) CK(cudaEventCreate(&e));
   p->info.dtype = p->dtype;
   p->info.format = p->format;
@@ -346,7 +347,9 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   std::snprintf(p->info.variant, sizeof p->info.variant, "%s/%s/%s/parts=%d/lanes=%s/V=%u%s%s", fm[p->format],
                 sc[p->scheme], sy[o.sync], o.nr_parts, o.lanes ? std::to_string(o.lanes).c_str() : "auto", p->V,
                 p->stage ? "/smem-x" : "", p->pipe ? "/tma-pipe" : "");
-  CK(cudaDeviceSynchronize());
+  // the uploads and clears above ran on the plan's stream: done before any
+  // launch, on any stream, can read them
+  CK(cudaStreamSynchronize(p->stream));
   return SPARSEP_OK;
 }
 
@@ -362,6 +365,10 @@ static int begin_plan(sparsep_plan **out, int dtype, int format, int scheme, con
   CK(cudaGetDevice(&dev));
   auto *p = new (std::nothrow) sparsep_plan();
   if (!p) return SPARSEP_ENOMEM;
+  if (cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking)) {
+    delete p;
+    return map_cuda(e);
+  }
   CK(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev));
   p->dtype = dtype;
   p->format = format;
@@ -1246,12 +1253,15 @@ static int run_any(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) 
   return SPARSEP_EINVAL;
 }
 
+// The error word after the plan's stream has drained; reset for the next run.
 static int check_err(sparsep_plan *p) {
   int e = 0;
-  CK(cudaMemcpy(&e, p->err, sizeof e, cudaMemcpyDeviceToHost));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaMemcpyAsync(&e, p->err, sizeof e, cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
   if (e) {
-    int z = 0;
-    cudaMemcpy(p->err, &z, sizeof z, cudaMemcpyHostToDevice);
+    CK(cudaMemsetAsync(p->err, 0, sizeof e, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
     return e;
   }
   return SPARSEP_OK;

@@ -142,8 +142,10 @@ def bcsr_triplets(B):
 
 
 def stratified_cols(rng, lens, lo, hi):
-    """Per row r, lens[r] distinct sorted columns in [lo[r], hi[r]): one uniform
-    draw inside each of lens[r] equal strata (no sort, no redraw needed)."""
+    """Per row r, lens[r] <= hi[r] - lo[r] distinct sorted columns in
+    [lo[r], hi[r]): one uniform draw inside each of the integer strata
+    [floor(i w / len), floor((i + 1) w / len)), w = hi - lo, which are disjoint
+    and non-empty (no sort, no redraw needed)."""
     lens = np.asarray(lens, dtype=np.int64)
     total = int(lens.sum())
     rowptr = np.zeros(lens.size + 1, dtype=np.int64)
@@ -151,8 +153,11 @@ def stratified_cols(rng, lens, lo, hi):
     row_of = np.repeat(np.arange(lens.size), lens)
     i = np.arange(total, dtype=np.int64) - rowptr[:-1][row_of]
     w = (hi - lo).astype(np.int64)[row_of]
-    u = rng.random(total)
-    col = lo[row_of] + np.floor((i + u) * w / lens[row_of]).astype(np.int64)
+    ln = lens[row_of]
+    a = i * w // ln
+    span = (i + 1) * w // ln - a
+    off = np.minimum(np.floor(rng.random(total) * span).astype(np.int64), span - 1)
+    col = lo[row_of] + a + off
     return rowptr.astype(np.uint32), col.astype(np.uint32)
 
 
@@ -194,3 +199,86 @@ def batch_workload(nmats=512, seed=3, dtype=np.float32, rows_lo=1_000, rows_hi=2
         x = rng.uniform(-1, 1, (n, k)).astype(dt) if dt.kind == "f" else rng.integers(-8, 9, (n, k)).astype(dt)
         out.append(dict(n=n, kind=kind, k=k, rowptr=rowptr, colind=cols, values=vals, x=x))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Training and held-out matrices of the learned variant selector
+# ---------------------------------------------------------------------------
+SELECTOR_FAMILIES = ("uniform", "zipf", "banded", "blockdiag", "rmat")
+
+
+def _rows_from_pairs(n, rows, cols):
+    """Distinct (row, col) pairs sorted by row then column -> rowptr, colind."""
+    key = np.unique(rows.astype(np.int64) * n + cols.astype(np.int64))
+    r = (key // n).astype(np.int64)
+    rowptr = np.zeros(n + 1, dtype=np.uint32)
+    np.cumsum(np.bincount(r, minlength=n), out=rowptr[1:])
+    return rowptr, (key % n).astype(np.uint32)
+
+
+def selector_matrix(rng, family: str, n: int, mean_len: float):
+    """One square training matrix (rowptr, colind) of a family:
+    uniform   row lengths uniform in [1, 2 mean_len - 1], columns anywhere;
+    zipf      power-law row lengths (exponent 2) scaled to mean_len;
+    banded    columns within a band of half-width 2-64 x mean_len;
+    blockdiag dense-ish diagonal blocks of 16-512 rows, columns inside the block;
+    rmat      R-MAT graph, quadrant probabilities a/b/c/d = 0.57/0.19/0.19/0.05,
+              n rounded to a power of two, about n * mean_len edges."""
+    lo = np.zeros(n, dtype=np.int64)
+    hi = np.full(n, n, dtype=np.int64)
+    m = max(1, int(round(mean_len)))
+    if family == "uniform":
+        lens = rng.integers(1, 2 * m, n)
+    elif family == "zipf":
+        z = rng.zipf(2.0, n).astype(np.float64)
+        lens = np.maximum(1, np.round(z * (m / z.mean()))).astype(np.int64)
+    elif family == "banded":
+        bw = int(m * rng.uniform(2, 64))
+        r = np.arange(n)
+        lo, hi = np.maximum(0, r - bw), np.minimum(n, r + bw + 1)
+        lens = rng.integers(max(1, m // 2), 2 * m, n)
+    elif family == "blockdiag":
+        bs = int(rng.choice([16, 32, 64, 128, 256, 512]))
+        r = np.arange(n)
+        lo = (r // bs) * bs
+        hi = np.minimum(n, lo + bs)
+        lens = rng.integers(max(1, m // 2), 2 * m, n)
+    elif family == "rmat":
+        scale = max(4, int(round(np.log2(n))))
+        n = 1 << scale
+        ne = n * m
+        rows = np.zeros(ne, dtype=np.int64)
+        cols = np.zeros(ne, dtype=np.int64)
+        a, b, c = 0.57, 0.19, 0.19
+        for _ in range(scale):
+            u = rng.random(ne)
+            rows = rows * 2 + (u >= a + b)
+            cols = cols * 2 + (((u >= a) & (u < a + b)) | (u >= a + b + c))
+        rp, ci = _rows_from_pairs(n, rows, cols)
+        return n, rp, ci
+    else:
+        raise ValueError(family)
+    lens = np.minimum(np.minimum(lens, hi - lo), 50_000)
+    rp, ci = stratified_cols(rng, lens, lo, hi)
+    return n, rp, ci
+
+
+def selector_one(seed: int, i: int, rows_lo=1_000, rows_hi=262_144, len_lo=2, len_hi=64, max_nnz=4_000_000,
+                 k_max=32):
+    """Training matrix i of the stream `seed` (its own generator, so any
+    subset can be built in any process): family in turn, rows and mean row
+    length log-uniform, k uniform in 1..k_max, nonzeros capped at max_nnz
+    (the row count shrinks to fit).  -> dict(family, n, rowptr, colind, k)."""
+    rng = np.random.default_rng([seed, i])
+    fam = SELECTOR_FAMILIES[i % len(SELECTOR_FAMILIES)]
+    n = int(np.exp(rng.uniform(np.log(rows_lo), np.log(rows_hi))))
+    ml = float(np.exp(rng.uniform(np.log(len_lo), np.log(len_hi))))
+    n = max(rows_lo // 2, min(n, int(max_nnz / ml)))
+    k = int(rng.integers(1, k_max + 1))
+    n, rp, ci = selector_matrix(rng, fam, n, ml)
+    return dict(family=fam, n=n, rowptr=rp, colind=ci, k=k)
+
+
+def selector_workload(count: int, seed: int, **kw):
+    """Training matrices 0 .. count - 1 of the stream `seed`."""
+    return [selector_one(seed, i, **kw) for i in range(count)]
