@@ -561,14 +561,17 @@ int sparsep_features(uint32_t nrows, uint32_t ncols, const uint32_t *rowptr, con
                      float *out);
 /* network primitives on device buffers: weights d_wb (BF16 bits, nparams),
  * standardised features d_x (n x 16), times d_t (n x K, 0 = variant does not
- * apply); loss_grad writes the mean expected-regret loss and its gradient
- * (d_scratch: sparsep_mlp_scratch_floats(n) floats); adam updates the FP32
- * master weights and their BF16 copy */
+ * apply); loss_grad writes the mean loss and its gradient: per matrix,
+ * (t_best * wscale)^alpha x (expected regret of a softmax pick + ce_weight x
+ * cross-entropy to softmax(-regret / tau)) (d_scratch:
+ * sparsep_mlp_scratch_floats(n) floats); adam updates the FP32 master
+ * weights and their BF16 copy */
 uint32_t sparsep_mlp_nparams(void);
 size_t sparsep_mlp_scratch_floats(uint32_t n);
 int sparsep_mlp_forward(const uint16_t *d_wb, const float *d_x, uint32_t n, float *d_logits, void *stream);
 int sparsep_mlp_loss_grad(const uint16_t *d_wb, const float *d_x, const float *d_t, uint32_t n, float wscale,
-                          float *d_grad, float *d_loss, float *d_scratch, void *stream);
+                          float alpha, float ce_weight, float tau, float *d_grad, float *d_loss, float *d_scratch,
+                          void *stream);
 int sparsep_mlp_adam(float *d_w, uint16_t *d_wb, const float *d_grad, float *d_m, float *d_v, uint32_t step,
                      float lr, float beta1, float beta2, float eps, float weight_decay, void *stream);
 int sparsep_mlp_to_bf16(const float *d_w, uint16_t *d_wb, void *stream);

@@ -8,7 +8,9 @@ network and objective from the same BF16 weights:
   W1[64][16], b1[64], W2[64][64], b2[64], W3[K][64], b3[K];
   per sample s over the variants c with t[s, c] > 0:
     p = softmax(z_s) over those c,  r_c = t_c / min t - 1,
-    L_s = w_s * sum_c p_c r_c,  w_s = min t * wscale,
+    q = softmax(-r / tau) over those c,
+    L_s = w_s * (sum_c p_c r_c + lam * sum_c -q_c log p_c),
+    w_s = (min t * wscale) ** alpha,
   loss = mean_s L_s (samples with no applicable variant count as 0).
 
 The selector has no counterpart in the reference; nothing here follows a
@@ -60,7 +62,8 @@ def forward(w: np.ndarray, x: np.ndarray, K: int):
     return h1, h2, z
 
 
-def loss_grad(w: np.ndarray, x: np.ndarray, t: np.ndarray, wscale: float):
+def loss_grad(w: np.ndarray, x: np.ndarray, t: np.ndarray, wscale: float, alpha: float = 1.0, lam: float = 0.0,
+              tau: float = 0.05):
     """Loss and its gradient w.r.t. the packed weights (all float64)."""
     n, K = t.shape
     w = np.asarray(w, dtype=np.float64)
@@ -77,9 +80,13 @@ def loss_grad(w: np.ndarray, x: np.ndarray, t: np.ndarray, wscale: float):
     tb = np.where(anyv, np.where(mask, t, np.inf).min(axis=1), 0.0)
     r = np.where(mask, t / np.where(anyv, tb, 1.0)[:, None] - 1.0, 0.0)
     er = (p * r).sum(axis=1)
-    ws = np.where(anyv, tb * wscale, 0.0)
-    loss = float((ws * er).sum() / n)
-    dz = (ws[:, None] * p * (r - er[:, None])) / n
+    eq = np.where(mask, np.exp(-r / tau), 0.0)
+    q = eq / np.where(anyv, eq.sum(axis=1), 1.0)[:, None]
+    logp = np.where(mask, z - zmax[:, None] - np.log(np.where(anyv, e.sum(axis=1), 1.0))[:, None], 0.0)
+    ce = -(q * logp).sum(axis=1)
+    ws = np.where(anyv, (np.where(anyv, tb, 1.0) * wscale) ** alpha, 0.0)
+    loss = float((ws * (er + lam * ce)).sum() / n)
+    dz = (ws[:, None] * (p * (r - er[:, None]) + lam * (p - q))) / n
     dz = np.where(mask, dz, 0.0)
     dW3 = dz.T @ h2
     db3 = dz.sum(axis=0)

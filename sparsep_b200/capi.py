@@ -435,8 +435,8 @@ def _batch_sigs(L):
     L.sparsep_mlp_scratch_floats.argtypes = [C.c_uint32]
     L.sparsep_mlp_scratch_floats.restype = C.c_size_t
     L.sparsep_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
-    L.sparsep_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p,
-                                        C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sparsep_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_float,
+                                        C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.sparsep_mlp_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                    C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
     L.sparsep_mlp_to_bf16.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]

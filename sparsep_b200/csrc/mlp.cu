@@ -9,10 +9,15 @@
 // Training objective, per sample s (one matrix with its right-hand-side
 // count), over the variants c that apply to it (t[s][c] > 0, the measured
 // time): p = softmax(z) restricted to those c, regret r_c = t_c / min_c t_c - 1,
-//   L_s = w_s * sum_c p_c r_c,     w_s = min_c t_c / (mean over samples),
-// i.e. the expected relative slowdown of a pick drawn from p, weighted by the
-// matrix's share of the run time; the loss is the mean over samples and
-// dL/dz_c = w_s p_c (r_c - sum_c' p_c' r_c') / n.
+// soft target q = softmax(-r / tau) over the same c,
+//   L_s = w_s * ( sum_c p_c r_c  +  lambda * sum_c -q_c log p_c ),
+//   w_s = (min_c t_c * wscale)^alpha   (wscale = 1 / mean of min_c t_c),
+// i.e. the expected relative slowdown of a pick drawn from p, plus a
+// cross-entropy toward the near-best variants that keeps the gradient alive
+// once p is sharp and leaves p's top probability meaningful as a confidence;
+// alpha weighs matrices by their share of run time (0: all alike).  The loss
+// is the mean over samples and
+//   dL/dz_c = w_s ( p_c (r_c - sum_c' p_c' r_c') + lambda (p_c - q_c) ) / n.
 //
 // One CTA of 64 threads takes 64 samples, one thread per sample for the
 // forward and backward passes (activations in shared memory, padded rows);
@@ -60,9 +65,9 @@ __device__ __forceinline__ Acts carve(float *sm) {
 
 template <bool GRAD>
 __global__ void __launch_bounds__(S) fwd_bwd(const __nv_bfloat16 *__restrict__ wb, const float *__restrict__ xin,
-                                             const float *__restrict__ tin, uint32_t n, float wscale,
-                                             float *__restrict__ logits, float *__restrict__ gpart,
-                                             float *__restrict__ lpart) {
+                                             const float *__restrict__ tin, uint32_t n, float wscale, float alpha,
+                                             float lambda, float tau, float *__restrict__ logits,
+                                             float *__restrict__ gpart, float *__restrict__ lpart) {
   extern __shared__ float sm[];
   const Acts a = carve(sm);
   const int tid = threadIdx.x;
@@ -107,19 +112,31 @@ __global__ void __launch_bounds__(S) fwd_bwd(const __nv_bfloat16 *__restrict__ w
     const float t = valid ? tin[(size_t)s * K + c] : 0.f;
     sum += t > 0.f ? expf(a.dz[c * LD + tid] - zmax) : 0.f;
   }
-  float er = 0.f;  // expected regret under p
+  const float lsum = logf(sum);
+  float er = 0.f, qsum = 0.f;  // expected regret under p; soft-target normaliser
   for (int c = 0; c < K; ++c) {
     const float t = valid ? tin[(size_t)s * K + c] : 0.f;
-    if (t > 0.f) er += expf(a.dz[c * LD + tid] - zmax) / sum * (t / tb - 1.f);
+    if (t > 0.f) {
+      er += expf(a.dz[c * LD + tid] - zmax) / sum * (t / tb - 1.f);
+      qsum += expf(-(t / tb - 1.f) / tau);
+    }
   }
-  const float ws = any ? tb * wscale : 0.f;
+  float ce = 0.f;  // sum_c -q_c log p_c
+  for (int c = 0; c < K; ++c) {
+    const float t = valid ? tin[(size_t)s * K + c] : 0.f;
+    if (t > 0.f) ce -= expf(-(t / tb - 1.f) / tau) / qsum * (a.dz[c * LD + tid] - zmax - lsum);
+  }
+  const float ws = any ? powf(tb * wscale, alpha) : 0.f;
   for (int c = 0; c < K; ++c) {
     const float t = valid ? tin[(size_t)s * K + c] : 0.f;
     float g = 0.f;
-    if (any && t > 0.f) g = ws * (expf(a.dz[c * LD + tid] - zmax) / sum) * ((t / tb - 1.f) - er) / (float)n;
+    if (any && t > 0.f) {
+      const float p = expf(a.dz[c * LD + tid] - zmax) / sum, r = t / tb - 1.f;
+      g = ws * (p * (r - er) + lambda * (p - expf(-r / tau) / qsum)) / (float)n;
+    }
     a.dz[c * LD + tid] = g;
   }
-  a.red[tid] = any ? ws * er / (float)n : 0.f;
+  a.red[tid] = any ? ws * (er + lambda * ce) / (float)n : 0.f;
 
   // backward through the hidden layers
   for (int j = 0; j < H; ++j) {
@@ -233,19 +250,20 @@ int sparsep_mlp_forward(const uint16_t *d_wb, const float *d_x, uint32_t n, floa
   if (!n) return SPARSEP_OK;
   if (int st = map_err(set_smem())) return st;
   fwd_bwd<false><<<(n + S - 1) / S, S, SMEM, static_cast<cudaStream_t>(stream)>>>(
-      reinterpret_cast<const __nv_bfloat16 *>(d_wb), d_x, nullptr, n, 0.f, d_logits, nullptr, nullptr);
+      reinterpret_cast<const __nv_bfloat16 *>(d_wb), d_x, nullptr, n, 0.f, 0.f, 0.f, 1.f, d_logits, nullptr, nullptr);
   return map_err(cudaGetLastError());
 }
 
 int sparsep_mlp_loss_grad(const uint16_t *d_wb, const float *d_x, const float *d_t, uint32_t n, float wscale,
-                          float *d_grad, float *d_loss, float *d_scratch, void *stream) {
-  if (!d_wb || !d_x || !d_t || !d_grad || !d_scratch || !n) return SPARSEP_EINVAL;
+                          float alpha, float ce_weight, float tau, float *d_grad, float *d_loss, float *d_scratch,
+                          void *stream) {
+  if (!d_wb || !d_x || !d_t || !d_grad || !d_scratch || !n || !(tau > 0.f)) return SPARSEP_EINVAL;
   if (int st = map_err(set_smem())) return st;
   const uint32_t nb = (n + S - 1) / S;
   float *gpart = d_scratch, *lpart = d_scratch + (size_t)nb * NP;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  fwd_bwd<true><<<nb, S, SMEM, st>>>(reinterpret_cast<const __nv_bfloat16 *>(d_wb), d_x, d_t, n, wscale, nullptr,
-                                     gpart, lpart);
+  fwd_bwd<true><<<nb, S, SMEM, st>>>(reinterpret_cast<const __nv_bfloat16 *>(d_wb), d_x, d_t, n, wscale, alpha,
+                                     ce_weight, tau, nullptr, gpart, lpart);
   if (int e = map_err(cudaGetLastError())) return e;
   reduce_parts<<<(NP + 1 + 255) / 256, 256, 0, st>>>(gpart, lpart, nb, d_grad, d_loss);
   return map_err(cudaGetLastError());

@@ -119,9 +119,12 @@ def standardise(feats: np.ndarray):
     return mean, std
 
 
-def train(feats: np.ndarray, times: np.ndarray, steps: int = 4000, lr: float = 3e-3, seed: int = 0,
-          weight_decay: float = 1e-4, log_every: int = 500, log=print) -> dict:
-    """Full-batch Adam on the expected-regret loss; returns the model dict."""
+def train(feats: np.ndarray, times: np.ndarray, steps: int = 3000, lr: float = 3e-3, seed: int = 0,
+          weight_decay: float = 1e-4, alpha: float = 0.5, ce_weight: float = 0.02, tau: float = 0.05,
+          log_every: int = 500, log=print) -> dict:
+    """Full-batch Adam on the selector loss (expected regret of a softmax pick
+    plus ce_weight x cross-entropy to softmax(-regret / tau), each matrix
+    weighted by (its best time / the mean)^alpha); returns the model dict."""
     import torch
 
     L = capi.lib()
@@ -147,8 +150,9 @@ def train(feats: np.ndarray, times: np.ndarray, steps: int = 4000, lr: float = 3
     capi.check(L.sparsep_mlp_to_bf16(w.data_ptr(), wb.data_ptr(), stream), "mlp_to_bf16")
     history = []
     for step in range(1, steps + 1):
-        capi.check(L.sparsep_mlp_loss_grad(wb.data_ptr(), X.data_ptr(), T.data_ptr(), n, wscale, g.data_ptr(),
-                                           loss.data_ptr(), scratch.data_ptr(), stream), "mlp_loss_grad")
+        capi.check(L.sparsep_mlp_loss_grad(wb.data_ptr(), X.data_ptr(), T.data_ptr(), n, wscale, alpha, ce_weight,
+                                           tau, g.data_ptr(), loss.data_ptr(), scratch.data_ptr(), stream),
+                   "mlp_loss_grad")
         if step == 1 or step % log_every == 0 or step == steps:
             history.append((step, float(loss.item())))
             if log:
@@ -217,7 +221,7 @@ def main(argv=None):
     g.add_argument("--out", type=Path, required=True)
     t = sub.add_parser("train")
     t.add_argument("--db", type=Path, nargs="+", required=True)
-    t.add_argument("--steps", type=int, default=4000)
+    t.add_argument("--steps", type=int, default=3000)
     t.add_argument("--lr", type=float, default=3e-3)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--heldout", type=Path)
@@ -236,7 +240,8 @@ def main(argv=None):
         feats = np.concatenate([d["feats"] for d in dbs])
         times = np.concatenate([d["times"] for d in dbs])
         model = train(feats, times, steps=a.steps, lr=a.lr, seed=a.seed)
-        meta = dict(train_samples=int(len(feats)), steps=a.steps, lr=a.lr, seed=a.seed,
+        meta = dict(train_samples=int(len(feats)), steps=a.steps, lr=a.lr, seed=a.seed, alpha=0.5, ce_weight=0.02,
+                    tau=0.05,
                     final_loss=float(model["history"][-1, 1]), db=[p.name for p in a.db])
         sel = selector(model)
         meta["train_eval"] = evaluate(sel.scores(feats), times, np.concatenate([d["meta"][:, 3] for d in dbs]))

@@ -65,14 +65,16 @@ def test_oracle_gradient_is_the_derivative():
     x = rng.normal(0, 1, (40, 16))
     t = np.where(rng.random((40, K)) < 0.6, rng.uniform(1, 5, (40, K)), 0.0)
     t[3] = 0.0  # a sample with no applicable variant
-    _, g = mo.loss_grad(w, x, t, 0.3)
-    eps = 1e-6
-    for i in rng.choice(NP, 60, replace=False):
-        wp, wm = w.copy(), w.copy()
-        wp[i] += eps
-        wm[i] -= eps
-        fd = (mo.loss_grad(wp, x, t, 0.3)[0] - mo.loss_grad(wm, x, t, 0.3)[0]) / (2 * eps)
-        assert abs(fd - g[i]) <= 1e-7 * max(1.0, np.abs(g).max()), i
+    for alpha, lam, tau in ((1.0, 0.0, 0.05), (0.5, 0.3, 0.1)):
+        _, g = mo.loss_grad(w, x, t, 0.3, alpha, lam, tau)
+        eps = 1e-6
+        for i in rng.choice(NP, 60, replace=False):
+            wp, wm = w.copy(), w.copy()
+            wp[i] += eps
+            wm[i] -= eps
+            fd = (mo.loss_grad(wp, x, t, 0.3, alpha, lam, tau)[0] - mo.loss_grad(wm, x, t, 0.3, alpha, lam, tau)[0]) / (
+                2 * eps)
+            assert abs(fd - g[i]) <= 1e-7 * max(1.0, np.abs(g).max()), (i, alpha, lam)
 
 
 def test_bf16_rounding_oracle():
@@ -98,7 +100,8 @@ def _dev_problem(n, seed):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 63, 200, 1000])
-def test_gpu_forward_and_gradient_match_oracle(n):
+@pytest.mark.parametrize("alpha,lam,tau", [(1.0, 0.0, 0.05), (0.5, 0.02, 0.05), (0.0, 0.5, 0.2)])
+def test_gpu_forward_and_gradient_match_oracle(n, alpha, lam, tau):
     """The CUDA forward logits and loss / gradient (FP32 accumulate) against
     the FP64 oracle evaluated at the same BF16 weights."""
     import torch
@@ -116,16 +119,16 @@ def test_gpu_forward_and_gradient_match_oracle(n):
     g = torch.zeros(NP, device="cuda")
     loss = torch.zeros(1, device="cuda")
     scratch = torch.zeros(int(L.sparsep_mlp_scratch_floats(n)), device="cuda")
-    capi.check(L.sparsep_mlp_loss_grad(dwb.data_ptr(), dx.data_ptr(), dt.data_ptr(), n, wscale, g.data_ptr(),
-                                       loss.data_ptr(), scratch.data_ptr(), None))
-    lo, go = mo.loss_grad(wq, x, t, wscale)
+    capi.check(L.sparsep_mlp_loss_grad(dwb.data_ptr(), dx.data_ptr(), dt.data_ptr(), n, wscale, alpha, lam, tau,
+                                       g.data_ptr(), loss.data_ptr(), scratch.data_ptr(), None))
+    lo, go = mo.loss_grad(wq, x, t, wscale, alpha, lam, tau)
     gg = g.cpu().numpy().astype(np.float64)
     assert abs(loss.item() - lo) <= 1e-4 * max(1.0, abs(lo))
     assert np.abs(gg - go).max() <= 1e-4 * max(np.abs(go).max(), 1e-12), np.abs(gg - go).max()
     # bit-identical on a second run (fixed-order reductions)
     g2 = torch.zeros_like(g)
-    capi.check(L.sparsep_mlp_loss_grad(dwb.data_ptr(), dx.data_ptr(), dt.data_ptr(), n, wscale, g2.data_ptr(),
-                                       loss.data_ptr(), scratch.data_ptr(), None))
+    capi.check(L.sparsep_mlp_loss_grad(dwb.data_ptr(), dx.data_ptr(), dt.data_ptr(), n, wscale, alpha, lam, tau,
+                                       g2.data_ptr(), loss.data_ptr(), scratch.data_ptr(), None))
     assert torch.equal(g, g2)
 
 
@@ -246,3 +249,14 @@ def test_trained_model_gain_on_heldout():
     assert res["regret_total"] <= 0.10, res
     assert res["speedup_vs_default"] > 1.0, res
     assert res["regret_total"] < res["default_regret_total"], res
+    # the confidence is informative: falling back below 0.3 lowers the regret
+    z = selector.selector(model).scores(h["feats"])
+    t = h["times"]
+    zz = np.where(t > 0, z, -np.inf)
+    p = np.exp(zz - zz.max(axis=1, keepdims=True))
+    conf = (p / p.sum(axis=1, keepdims=True)).max(axis=1)
+    best = np.where(t > 0, t, np.inf).min(axis=1)
+    pick = t[np.arange(len(t)), selector.picks(z, t)]
+    fb = conf < 0.3
+    assert 0.0 < fb.mean() < 0.5
+    assert np.where(fb, best, pick).sum() / best.sum() - 1 < res["regret_total"]
