@@ -10,7 +10,12 @@ One step = one SpMV over the whole matrix (inputs resident in HBM).  The L2
 step is timed with CUDA events on the launching stream.  `value` is
 compulsory bytes / device time summed over all ranks' steps (replicas, weak
 scaling).  `e2e` is the same metric through sparsep_execute_host: pinned host
-x in, pinned host y out, copies inside the timed region.
+x in, pinned host y out, copies inside the timed region.  `clocks` is sampled
+through NVML every millisecond during the timed region.
+
+`batched` (one GPU): the batched multi-RHS path on 512 matrices -- plain
+per-matrix launches against the one-launch work queue with the default,
+learned (sparsep_batch_select) and exhaustively autotuned variants.
 
 --impl reference times the reference's own host SpMV (spmv_host of
 spmv/1D/CSR-row/host/app.c, compiled from the reference sources into
@@ -67,48 +72,75 @@ def compulsory_bytes(n, m, nnz, s=4):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled through NVML (read-only
+    queries) every millisecond by a thread during the timed region."""
+    REASONS = (("nvmlClocksEventReasonHwSlowdown", "hw_slowdown"),
+               ("nvmlClocksEventReasonHwThermalSlowdown", "hw_thermal_slowdown"),
+               ("nvmlClocksEventReasonSwThermalSlowdown", "sw_thermal_slowdown"),
+               ("nvmlClocksEventReasonSwPowerCap", "sw_power_cap"))
 
     def __init__(self, dev):
         self.dev = dev
-        self.p = None
+        self.rows = []
+        self.err = None
+
+    def _handle(self):
+        import pynvml as nv
+        import torch
+
+        nv.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return nv, nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv, nv.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _sample(self):
+        sm = self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+        r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        self.rows.append((sm, [name for bit, name in self.bits if r & bit]))
+
+    def _run(self):
+        try:
+            while not self.stop.is_set():
+                self._sample()
+                self.stop.wait(0.001)
+        except Exception as e:
+            self.err = repr(e)
 
     def __enter__(self):
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
-                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.p = None
+        import threading
+
+        self.stop = threading.Event()
+        self.t = None
+        try:  # NVML set up (and one sample taken) before the timed region starts
+            self.nv, self.h = self._handle()
+            self.max_mhz = self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+            self.bits = [(getattr(self.nv, k), name) for k, name in self.REASONS]
+            self._sample()
+        except Exception as e:  # no NVML: reported, not fatal
+            self.err = repr(e)
+            return self
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
         return self
 
     def __exit__(self, *a):
-        self.out = ""
-        if self.p:
-            self.p.terminate()
-            try:
-                self.out, _ = self.p.communicate(timeout=5)
-            except Exception:
-                self.p.kill()
+        self.stop.set()
+        if self.t:
+            self.t.join(timeout=5)
+        try:
+            self._sample()  # one more after the last timed step
+        except Exception:
+            pass
 
     def summary(self):
-        rows = []
-        for ln in (getattr(self, "out", "") or "").splitlines():
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) >= 9:
-                try:
-                    rows.append((float(f[1]), float(f[2]), f[5:9]))
-                except ValueError:
-                    pass
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "error": self.err}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted({x for _, rs in self.rows for x in rs}), "samples": len(self.rows),
+                "source": "nvml"}
 
 
 def run_ours(args, rank, world):
@@ -220,6 +252,78 @@ def run_ours(args, rank, world):
                                            threads=1)
     plan.free()
     return res
+
+
+def run_batch(args):
+    """The batched multi-RHS path (FP32) on the 512-matrix workload: plain
+    per-matrix launches (default variant per matrix) against the one-launch
+    queue with the default, learned and exhaustively autotuned variants.
+    The batch's compulsory bytes (8.9 GB) exceed L2 many times over, so no
+    flush is needed between timed runs."""
+    import torch
+
+    import sparsep_b200 as sp
+    from sparsep_b200 import capi, selector
+
+    t0 = time.time()
+    w = sp.synth.batch_workload(nmats=args.batch_mats, dtype=np.float32)
+    mats = [sp.csr("f32", d["n"], d["n"], d["rowptr"], d["colind"], d["values"]) for d in w]
+    b = capi.Batch("f32", mats, [d["k"] for d in w])
+    for m, d in enumerate(w):
+        b.set_x(m, d["x"])
+    setup_s = time.time() - t0
+    info = b.info()
+    cb = info["compulsory_bytes"]
+    st = torch.cuda.Stream()
+
+    def timeit(fn, reps=5):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    sample = list(range(0, len(w), max(1, len(w) // 24)))
+    plain = timeit(lambda: b.execute_per_matrix(st.cuda_stream))
+    y_plain = {m: b.get_y(m) for m in sample}
+    default = timeit(lambda: b.execute(st.cuda_stream))
+    sel = selector.selector(selector.load())
+    t0 = time.time()
+    b.select(sel, min_confidence=0.0)
+    select_s = time.time() - t0
+    learned = timeit(lambda: b.execute(st.cuda_stream))
+    b.status()
+    dev = max(float(np.abs(b.get_y(m) - y_plain[m]).max() / max(np.abs(y_plain[m]).max(), 1e-30)) for m in sample)
+    t0 = time.time()
+    b.autotune(reps=3)
+    tune_s = time.time() - t0
+    tuned = timeit(lambda: b.execute(st.cuda_stream))
+    b.status()
+    b.free()
+
+    def gbs(ms):
+        return round(cb / (ms * 1e-3) / 1e9, 2)
+
+    return {"workload": f"{len(w)} CSR matrices, rows log-uniform 1k-256k, uniform / Zipf / banded, 1-32 "
+                        "right-hand sides each, FP32 (seed 3)",
+            "nnz": int(info["nnz"]), "compulsory_bytes": int(cb), "items": int(info["items"]),
+            "plain_per_matrix_ms": round(plain, 3), "queue_default_ms": round(default, 3),
+            "queue_learned_ms": round(learned, 3), "queue_autotuned_ms": round(tuned, 3),
+            "learned_speedup_vs_plain": round(plain / learned, 3),
+            "learned_over_autotuned": round(learned / tuned, 4),
+            "gbs": {"plain": gbs(plain), "default": gbs(default), "learned": gbs(learned), "autotuned": gbs(tuned)},
+            "select_s": round(select_s, 3), "autotune_s": round(tune_s, 2), "setup_s": round(setup_s, 1),
+            "learned_max_rel_diff_vs_plain": dev,
+            "accuracy": "FP32 sums per row in a variant-dependent order; every variant is within the per-row "
+                        "gamma bound (tests); INT32 bit-exact",
+            "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
 
 
 def _ref_csr_lib():
@@ -342,11 +446,14 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default="all", choices=["all", "single", "batch"],
+                    help="single: the FP32 CSR Zipf SpMV only; batch: the batched path only")
+    ap.add_argument("--batch-mats", type=int, default=512)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -362,7 +469,17 @@ def main():
         if args.impl == "ours":
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    res = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    elif args.only == "batch":
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        res = {"batched": run_batch(args)} if rank == 0 else None
+    else:
+        res = run_ours(args, rank, world)
+        if args.only == "all" and world == 1:
+            res["batched"] = run_batch(args)
     if world > 1 and args.impl == "ours":
         import torch.distributed as dist
 
