@@ -290,6 +290,25 @@ def coo(dtype: str, nrows: int, ncols: int, rows, cols, vals) -> HostMatrix:
     return HostMatrix("coo", dtype, s, {"rowindx": r, "colind": c, "values": v})
 
 
+def bcsr(dtype: str, nrows: int, ncols: int, rb: int, cb: int, browptr, bcolind, bval, nnz: int,
+         nnz_per_block=None) -> HostMatrix:
+    """A BCSR struct over existing block arrays (block rows of rb x cb dense
+    blocks sorted by block column, bval row-major per block), as the
+    reference's csr2bcsr + sortBCSRMatrix + countNNZperBlockBCSRMatrix leave it."""
+    dt = DTYPES[dtype]
+    nbr = (nrows + rb - 1) // rb
+    bp = _pad(np.ascontiguousarray(browptr, dtype=np.uint32), 1)
+    bc = _pad(np.ascontiguousarray(bcolind, dtype=np.uint32), 1)
+    bv = _pad(np.ascontiguousarray(np.asarray(bval).reshape(-1), dtype=dt.np), 1)
+    nb = int(bp[nbr])
+    if nnz_per_block is None:
+        nnz_per_block = (np.asarray(bval).reshape(nb, -1) != 0).sum(axis=1) if nb else np.zeros(0)
+    npb = _pad(np.ascontiguousarray(nnz_per_block, dtype=np.uint32), 1)
+    s = STRUCTS[dtype]["bcsr"](rb, cb, nbr, (ncols + cb - 1) // cb, nb, nrows % rb, nrows, ncols, nnz,
+                               ptr(bp, C.c_uint32), ptr(bc, C.c_uint32), ptr(bv, dt.ct), ptr(npb, C.c_uint32))
+    return HostMatrix("bcsr", dtype, s, {"browptr": bp, "bcolind": bc, "bval": bv, "nnz_per_block": npb})
+
+
 def convert(name: str, A: HostMatrix, *args: int) -> HostMatrix:
     a, b, nx = CONVERTERS[name]
     assert A.kind == a and len(args) == nx, (A.kind, name, args)

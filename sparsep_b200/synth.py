@@ -90,43 +90,52 @@ def to_csr(nrows, rows, cols, vals):
     return rowptr, cols.astype(np.uint32), vals
 
 
-def block_banded(nrows=2_097_152, rb=4, cb=4, half_bw=32, p_block=0.3, p_fill=0.6, seed=2, dtype=np.int8):
+def block_banded(nrows=2_097_152, rb=4, cb=4, half_bw=32, p_block=0.3, p_fill=0.6, seed=2, dtype=np.int8,
+                 chunk=16_384):
     """Block-banded matrix built directly as BCSR arrays.
 
-    Returns dict with nrows, ncols, browptr, bcolind, bval (nblocks x rb x cb,
-    zeros at unfilled positions), nnz (filled positions), nnz_per_block
-    (nonzero values, as the reference's countNNZperBlockBCSRMatrix) and x.
+    Generated in chunks of `chunk` block rows (one generator, drawn in chunk
+    order), so the full 2M-row 8x8 case stays within a few GB.  Returns dict
+    with nrows, ncols, browptr, bcolind, bval (nblocks x rb x cb, zeros at
+    unfilled positions), nnz (filled positions), nnz_per_block (nonzero
+    values, as the reference's countNNZperBlockBCSRMatrix) and x.
     """
     rng = np.random.default_rng(seed)
     ncols = nrows
     nbr = (nrows + rb - 1) // rb
     nbc = (ncols + cb - 1) // cb
     width = 2 * half_bw + 1
-    present = rng.random((nbr, width)) < p_block
-    jj = np.arange(nbr)[:, None] - half_bw + np.arange(width)[None, :]
-    present &= (jj >= 0) & (jj < nbc)
-    counts = present.sum(axis=1)
-    browptr = np.zeros(nbr + 1, dtype=np.uint32)
-    np.cumsum(counts, out=browptr[1:])
-    bcolind = jj[present].astype(np.uint32)  # row-major -> sorted by column within a block row
-    nb = bcolind.size
-    fill = rng.random((nb, rb, cb)) < p_fill
-    # rows / cols past the matrix edge stay empty
-    brow_of = np.repeat(np.arange(nbr), counts)
-    r_ok = (brow_of[:, None] * rb + np.arange(rb)[None, :]) < nrows
-    c_ok = (bcolind[:, None].astype(np.int64) * cb + np.arange(cb)[None, :]) < ncols
-    fill &= r_ok[:, :, None] & c_ok[:, None, :]
     dt = np.dtype(dtype)
-    if dt.kind == "f":
-        v = rng.uniform(-1.0, 1.0, (nb, rb, cb)).astype(dt)
-    else:
-        v = rng.integers(-4, 5, (nb, rb, cb)).astype(dt)
-    bval = np.where(fill, v, dt.type(0)).astype(dt)
-    nnz = int(fill.sum())
-    nnz_per_block = (bval != 0).reshape(nb, -1).sum(axis=1).astype(np.uint32)
+    counts, bcols, bvals, npbs = [], [], [], []
+    nnz = 0
+    for b0 in range(0, nbr, chunk):
+        b1 = min(nbr, b0 + chunk)
+        present = rng.random((b1 - b0, width), dtype=np.float32) < p_block
+        jj = np.arange(b0, b1)[:, None] - half_bw + np.arange(width)[None, :]
+        present &= (jj >= 0) & (jj < nbc)
+        counts.append(present.sum(axis=1))
+        bc = jj[present].astype(np.uint32)  # row-major -> sorted by column within a block row
+        nb = bc.size
+        brow = np.repeat(np.arange(b0, b1), counts[-1])
+        fill = rng.random((nb, rb, cb), dtype=np.float32) < p_fill
+        # rows / cols past the matrix edge stay empty
+        fill &= ((brow[:, None] * rb + np.arange(rb)[None, :]) < nrows)[:, :, None]
+        fill &= ((bc[:, None].astype(np.int64) * cb + np.arange(cb)[None, :]) < ncols)[:, None, :]
+        if dt.kind == "f":
+            v = rng.uniform(-1.0, 1.0, (nb, rb, cb)).astype(dt)
+        else:
+            v = rng.integers(-4, 5, (nb, rb, cb), dtype=np.int8).astype(dt)
+        v[~fill] = 0
+        nnz += int(fill.sum())
+        bcols.append(bc)
+        bvals.append(v)
+        npbs.append((v != 0).reshape(nb, -1).sum(axis=1).astype(np.uint32))
+    browptr = np.zeros(nbr + 1, dtype=np.uint32)
+    np.cumsum(np.concatenate(counts), out=browptr[1:])
+    bval = np.concatenate(bvals) if bvals else np.zeros((0, rb, cb), dt)
     x = rng.uniform(-1.0, 1.0, ncols).astype(dt) if dt.kind == "f" else rng.integers(-4, 5, ncols).astype(dt)
-    return dict(nrows=nrows, ncols=ncols, rb=rb, cb=cb, nbr=nbr, nbc=nbc, browptr=browptr, bcolind=bcolind,
-                bval=bval, nnz=nnz, nnz_per_block=nnz_per_block, x=x, fill=fill)
+    return dict(nrows=nrows, ncols=ncols, rb=rb, cb=cb, nbr=nbr, nbc=nbc, browptr=browptr,
+                bcolind=np.concatenate(bcols), bval=bval, nnz=nnz, nnz_per_block=np.concatenate(npbs), x=x)
 
 
 def bcsr_triplets(B):
