@@ -60,10 +60,11 @@ template <typename T> struct Staged {
 };
 
 // Index guards: a failed check records its site code in the error word
-// (read by sparsep_batch_status) and the guarded access is skipped, so a
-// corrupted item or column index cannot take the GPU down.  The cheap ones
-// (per item, per gathered column) are always on; the checked build
-// (-DSPARSEP_CHECK) adds a full scan of each staged rowptr slice.
+// (read by sparsep_batch_status) and the guarded work is skipped, so a
+// corrupted item or column index cannot take the GPU down.  The per-item ones
+// (staging windows, staged rowptr ends, every staged column inside x) are
+// always on; the checked build (-DSPARSEP_CHECK) adds a full scan of each
+// staged rowptr slice.
 __device__ __forceinline__ bool bchk(bool ok, int *err, int code) {
   if (!ok && err) atomicCAS(err, 0, code);
   return ok;
@@ -185,6 +186,17 @@ __device__ __forceinline__ bool landed(uint64_t *bar, uint32_t parity, int *err)
   return true;
 }
 
+// Every staged column index below ncols (and `ok` on every thread): the gather
+// loops read x without per-load checks.  One pass over the staged chunk, shared
+// by all lanes; the result is the same on every thread of the CTA.
+__device__ __forceinline__ bool staged_ok(const uint32_t *col, uint32_t n, uint32_t ncols, bool ok, int *err,
+                                          int code) {
+  bool cols = true;
+  for (uint32_t q = threadIdx.x; q < n; q += BT) cols &= col[q] < ncols;
+  ok = ok && bchk(cols, err, code);
+  return !__syncthreads_or(!ok);
+}
+
 // ---------------------------------------------------------------------------
 // Row arithmetic
 // ---------------------------------------------------------------------------
@@ -202,18 +214,12 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &
                                           uint32_t e, int gl) {
   constexpr int U = 16 / (V * ACC) > 2 ? 16 / (V * ACC) : 2;
   const uint32_t k = m.k;
-  if (!bchk(q <= e && e <= s.n, s.err, -2101)) return;
-  // columns are clamped into x (in bounds whatever the staged data); a clamp
-  // that changed a column is recorded once for the range
-  const uint32_t cmax = m.ncols - 1;
-  uint32_t bad = 0;
+  if (!bchk(q <= e && e <= s.n, s.err, -2101)) return;  // staged columns were checked against x once
   for (; q + U <= e; q += U) {
     uint32_t c[U];
     T v[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) c[u] = s.col[q + u], v[u] = s.val[q + u];
-#pragma unroll
-    for (int u = 0; u < U; ++u) bad |= c[u] > cmax, c[u] = min(c[u], cmax);
     VecT<T, V> xv[U][ACC];
 #pragma unroll
     for (int a = 0; a < ACC; ++a) {
@@ -233,9 +239,7 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &
     }
   }
   for (; q < e; ++q) {
-    const uint32_t cq = min(s.col[q], cmax);
-    bad |= s.col[q] > cmax;
-    const T *xr = m.x + (size_t)cq * k;
+    const T *xr = m.x + (size_t)s.col[q] * k;
     const T v = s.val[q];
 #pragma unroll
     for (int a = 0; a < ACC; ++a) {
@@ -247,7 +251,6 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &
       }
     }
   }
-  bchk(!bad, s.err, -2106);
 }
 
 template <typename T, int G, int V, int ACC>
@@ -368,7 +371,7 @@ __device__ __forceinline__ void item_long(const View<T> &m, const BItem &it, BSh
   const uint32_t k = m.k;
   A acc[ACC][1];
   zero_acc<T, 1, ACC>(acc);
-  uint32_t parity = 0, bad = 0;
+  uint32_t parity = 0;
   for (uint32_t c0 = it.p0; c0 < it.p1; c0 += BCAP, parity ^= 1u) {
     const uint32_t n = min(BCAP, it.p1 - c0);
     const Window wc = window(it.colind, c0, c0 + n, 4), wv = window(it.val, c0, c0 + n, sizeof(T));
@@ -377,10 +380,9 @@ __device__ __forceinline__ void item_long(const View<T> &m, const BItem &it, BSh
     if (tid == 0) issue(&sh.bar, sh.col, wc, sh.val, wv, nullptr, Window{0, 0, 0});
     if (!landed(&sh.bar, parity, err)) return;
     const Staged<T> s{nullptr, sh.col + wc.lead, sh.val + wv.lead, n, err};
+    if (!staged_ok(s.col, n, m.ncols, true, err, -2107)) return;
     for (uint32_t q = gi; q < n; q += NG) {
-      const uint32_t cq = min(s.col[q], m.ncols - 1);
-      bad |= s.col[q] >= m.ncols;
-      const T *xr = m.x + (size_t)cq * k;
+      const T *xr = m.x + (size_t)s.col[q] * k;
       const T v = s.val[q];
 #pragma unroll
       for (int a = 0; a < ACC; ++a) {
@@ -389,7 +391,6 @@ __device__ __forceinline__ void item_long(const View<T> &m, const BItem &it, BSh
       }
     }
   }
-  bchk(!bad, err, -2107);
   __syncthreads();
   A *red = reinterpret_cast<A *>(sh.col);
 #pragma unroll
@@ -468,7 +469,7 @@ __device__ __forceinline__ void long_acc(const View<T> &m, const BItem &it, BSha
 // runs one.)  Without a ticket counter, CTA b runs item i0 + b (one matrix's
 // items: the per-matrix launches and the autotuner's timing runs).
 template <typename T>
-__global__ void __launch_bounds__(BT) batch_items(const BItem *items, uint32_t i0, unsigned int *head, int *err) {
+__global__ void __launch_bounds__(BT, 4) batch_items(const BItem *items, uint32_t i0, unsigned int *head, int *err) {
   __shared__ BShared<T> sh;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -501,12 +502,13 @@ __global__ void __launch_bounds__(BT) batch_items(const BItem *items, uint32_t i
   if (!landed(&sh.bar, 0, err)) return;
   const Staged<T> s{sh.rp + wr.lead, sh.col + wc.lead, sh.val + wv.lead, it.p1 - it.p0, err};
   {
-    // the staged rowptr must run from p0 to p1 (checked build: non-decreasing)
-    bool ok = s.rp[0] == it.p0 && s.rp[it.nr] == it.p1;
+    // the staged rowptr must run from p0 to p1 (checked build: non-decreasing),
+    // and every staged column must lie inside x
+    bool rp_ok = s.rp[0] == it.p0 && s.rp[it.nr] == it.p1;
 #ifdef SPARSEP_CHECK
-    for (uint32_t i = tid; i < it.nr; i += BT) ok = ok && s.rp[i] <= s.rp[i + 1];
+    for (uint32_t i = tid; i < it.nr; i += BT) rp_ok = rp_ok && s.rp[i] <= s.rp[i + 1];
 #endif
-    if (__syncthreads_or(!bchk(ok, err, -2105))) return;
+    if (!staged_ok(s.col, it.p1 - it.p0, it.ncols, bchk(rp_ok, err, -2105), err, -2106)) return;
   }
   if (it.mode == MODE_ROWS) by_lanes<T, MODE_ROWS>(m, s, it, sh, tid);
   else by_lanes<T, MODE_MERGE>(m, s, it, sh, tid);
