@@ -385,6 +385,9 @@ void *sparsep_plan_y(sparsep_plan *plan);
  *   sparsep_read_coo_S(file, &coo)      readCOOMatrix, SoA, pads nrows/ncols to 8/sizeof(T)
  *                                       (spmv/1D/CSR-row/support/matrix.h:44-96)
  *   sparsep_read_coo_nopad_S(file, &coo) same without padding (spmv/1D/BCSR-nnz/support/matrix.h:63-110)
+ *   sparsep_read_mtx_values_S(file, &coo) no reference counterpart: the file's
+ *     own values (real / integer / pattern = 1), symmetric and skew-symmetric
+ *     files expanded, no padding; ENOSYS for complex, hermitian or array files
  *   sparsep_read_cooe_S(file, &cooe)    readCOOMatrix, AoS (spmv/1D/COO-nnz/support/matrix.h:31-83)
  *   sparsep_sort_cooe_S(cooe)           sortCOOMatrix (spmv/1D/COO-nnz/support/matrix.h:88-125)
  *   sparsep_coo2csr_S(coo, &csr)        coo2csr (spmv/1D/CSR-row/support/matrix.h:113-152)
@@ -427,6 +430,7 @@ void *sparsep_plan_y(sparsep_plan *plan);
   SPARSEP_DECLARE_KIND(T, S, bdbcoo)                                                     \
   int sparsep_read_coo_##S(const char *file, sparsep_coo_##S **out);                     \
   int sparsep_read_coo_nopad_##S(const char *file, sparsep_coo_##S **out);               \
+  int sparsep_read_mtx_values_##S(const char *file, sparsep_coo_##S **out);             \
   int sparsep_read_cooe_##S(const char *file, sparsep_cooe_##S **out);                   \
   int sparsep_sort_cooe_##S(sparsep_cooe_##S *A);                                        \
   int sparsep_coo2csr_##S(const sparsep_coo_##S *A, sparsep_csr_##S **out);              \

@@ -319,7 +319,7 @@ def convert(name: str, A: HostMatrix, *args: int) -> HostMatrix:
 
 def read_mtx(path: str, dtype: str, flavour: str = "coo") -> HostMatrix:
     kind = "cooe" if flavour == "cooe" else "coo"
-    fn = {"coo": "read_coo", "coo_nopad": "read_coo_nopad", "cooe": "read_cooe"}[flavour]
+    fn = {"coo": "read_coo", "coo_nopad": "read_coo_nopad", "cooe": "read_cooe", "values": "read_mtx_values"}[flavour]
     out = C.POINTER(STRUCTS[dtype][kind])()
     check(getattr(lib(), f"sparsep_{fn}_{dtype}")(str(path).encode(), C.byref(out)), fn)
     return HostMatrix(kind, dtype, out.contents, {}, owned_by_lib=True)

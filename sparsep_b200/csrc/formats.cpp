@@ -9,6 +9,10 @@
 // spmv/1D/CSR-row/support/matrix.h:121) so reference code that reads the
 // padding keeps working on our structs.
 #include <algorithm>
+#include <type_traits>
+#include <new>
+#include <cmath>
+#include <cctype>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -88,6 +92,145 @@ static int read_mtx(const char *file, MtxEntries &m) {
   std::fclose(fp);
   if (st == SPARSEP_OK && (!header || i != m.nnz)) st = SPARSEP_EBADF;
   return st;
+}
+
+// ---------------------------------------------------------------------------
+// Matrix Market with values (no reference counterpart: the reference reader
+// above replaces every value by rand()%4+1).  Coordinate format; real /
+// double / integer / pattern fields; general / symmetric / skew-symmetric
+// (off-diagonal entries mirrored, negated for skew).  A file without a banner
+// is read as real general.  Integer element types take the value rounded to
+// the nearest integer, wrapped to the type's width.
+// ---------------------------------------------------------------------------
+struct MtxValues {
+  uint32_t nrows = 0, ncols = 0;
+  std::vector<uint32_t> r, c;
+  std::vector<double> v;
+};
+
+static bool ieq(const char *a, const char *b) {
+  for (; *a && *b; ++a, ++b)
+    if (std::tolower((unsigned char)*a) != std::tolower((unsigned char)*b)) return false;
+  return *a == *b;
+}
+
+static int read_mtx_values(const char *file, MtxValues &m) {
+  if (!file) return SPARSEP_EINVAL;
+  FILE *fp = std::fopen(file, "r");
+  if (!fp) return SPARSEP_EBADF;
+  char line[4096];
+  bool header = false, first = true, pattern = false, sym = false, skew = false;
+  uint64_t want = 0, got = 0;
+  int st = SPARSEP_OK;
+  while (st == SPARSEP_OK && std::fgets(line, sizeof line, fp) != nullptr) {
+    if (first && std::strncmp(line, "%%MatrixMarket", 14) == 0) {
+      char *save = nullptr, *t[5] = {};
+      t[0] = strtok_r(line, " \t\r\n", &save);
+      for (int i = 1; i < 5; ++i) t[i] = strtok_r(nullptr, " \t\r\n", &save);
+      first = false;
+      if (!t[1] || !t[2] || !t[3] || !t[4] || !ieq(t[1], "matrix")) {
+        st = SPARSEP_EBADF;
+        break;
+      }
+      if (!ieq(t[2], "coordinate")) { st = SPARSEP_ENOSYS; break; }  // dense array format
+      if (ieq(t[3], "pattern")) pattern = true;
+      else if (!ieq(t[3], "real") && !ieq(t[3], "double") && !ieq(t[3], "integer")) { st = SPARSEP_ENOSYS; break; }
+      if (ieq(t[4], "symmetric")) sym = true;
+      else if (ieq(t[4], "skew-symmetric")) sym = skew = true;
+      else if (!ieq(t[4], "general")) { st = SPARSEP_ENOSYS; break; }  // hermitian
+      continue;
+    }
+    first = false;
+    char *p = line;
+    while (*p == ' ' || *p == '\t') ++p;
+    if (*p == '%' || *p == '\n' || *p == '\r' || *p == 0) continue;
+    char *end = nullptr;
+    if (!header) {
+      const long long a = std::strtoll(p, &end, 10), b = std::strtoll(end, &end, 10), c = std::strtoll(end, &end, 10);
+      if (a < 0 || b < 0 || c < 0 || a > 0xFFFFFFF0LL || b > 0xFFFFFFF0LL || c > 0xFFFFFFF0LL) {
+        st = SPARSEP_EBADF;
+        break;
+      }
+      m.nrows = (uint32_t)a;
+      m.ncols = (uint32_t)b;
+      want = (uint64_t)c;
+      const uint64_t cap = sym ? 2 * want : want;
+      if (cap > 0xFFFFFFF0ull) { st = SPARSEP_ERANGE; break; }
+      m.r.reserve(cap);
+      m.c.reserve(cap);
+      m.v.reserve(cap);
+      header = true;
+      continue;
+    }
+    const long long rr = std::strtoll(p, &end, 10);
+    char *e2 = nullptr;
+    const long long cc = std::strtoll(end, &e2, 10);
+    if (e2 == end || rr < 1 || cc < 1 || (uint64_t)rr > m.nrows || (uint64_t)cc > m.ncols || got >= want) {
+      st = SPARSEP_EBADF;
+      break;
+    }
+    double v = 1.0;
+    if (!pattern) {
+      char *e3 = nullptr;
+      v = std::strtod(e2, &e3);
+      if (e3 == e2) { st = SPARSEP_EBADF; break; }
+    }
+    m.r.push_back((uint32_t)(rr - 1));
+    m.c.push_back((uint32_t)(cc - 1));
+    m.v.push_back(v);
+    if (sym && rr != cc) {
+      if ((uint64_t)cc > m.nrows || (uint64_t)rr > m.ncols) { st = SPARSEP_EBADF; break; }
+      m.r.push_back((uint32_t)(cc - 1));
+      m.c.push_back((uint32_t)(rr - 1));
+      m.v.push_back(skew ? -v : v);
+    }
+    ++got;
+  }
+  std::fclose(fp);
+  if (st == SPARSEP_OK && (!header || got != want)) st = SPARSEP_EBADF;
+  return st;
+}
+
+template <typename T> static T from_double(double v) {
+  if constexpr (std::is_floating_point<T>::value) {
+    return (T)v;
+  } else {
+    return (T)(typename std::make_unsigned<T>::type)(unsigned long long)std::llround(v);  // wraps
+  }
+}
+
+template <typename T>
+int read_coo_values(const char *file, typename Types<T>::coo **out) {
+  if (!out) return SPARSEP_EINVAL;
+  *out = nullptr;
+  MtxValues m;
+  int st;
+  try {
+    st = read_mtx_values(file, m);
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
+  }
+  if (st) return st;
+  const uint32_t nnz = (uint32_t)m.r.size();
+  auto *A = xcalloc<typename Types<T>::coo>(1);
+  if (!A) return SPARSEP_ENOMEM;
+  A->nrows = m.nrows;
+  A->ncols = m.ncols;
+  A->nnz = nnz;
+  A->rowindx = xcalloc<uint32_t>(nnz ? nnz : 1);
+  A->colind = xcalloc<uint32_t>(nnz ? nnz : 1);
+  A->values = xcalloc<T>(nnz ? nnz : 1);
+  if (!A->rowindx || !A->colind || !A->values) {
+    free_coo<T>(A);
+    return SPARSEP_ENOMEM;
+  }
+  for (uint32_t i = 0; i < nnz; ++i) {
+    A->rowindx[i] = m.r[i];
+    A->colind[i] = m.c[i];
+    A->values[i] = from_double<T>(m.v[i]);
+  }
+  *out = A;
+  return SPARSEP_OK;
 }
 
 static uint32_t pad_dim(uint32_t n, size_t s) {
@@ -992,6 +1135,7 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t nbr, const ui
   int sparsep_read_coo_##S(const char *f, sparsep_coo_##S **o) { return read_coo<T>(f, true, o); }      \
   int sparsep_read_coo_nopad_##S(const char *f, sparsep_coo_##S **o) { return read_coo<T>(f, false, o); } \
   int sparsep_read_cooe_##S(const char *f, sparsep_cooe_##S **o) { return read_cooe<T>(f, o); }         \
+  int sparsep_read_mtx_values_##S(const char *f, sparsep_coo_##S **o) { return read_coo_values<T>(f, o); } \
   int sparsep_sort_cooe_##S(sparsep_cooe_##S *A) { return sort_cooe<T>(A); }                            \
   int sparsep_coo2csr_##S(const sparsep_coo_##S *A, sparsep_csr_##S **o) { return coo2csr<T>(A, o); }   \
   int sparsep_csr2bcsr_##S(const sparsep_csr_##S *A, uint32_t rb, uint32_t cb, sparsep_bcsr_##S **o) {  \
