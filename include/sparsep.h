@@ -550,6 +550,23 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
 
 /* ------------------------------------------------------------------------ */
+/* Conjugate gradient on a plan (no reference counterpart)                   */
+/* ------------------------------------------------------------------------ */
+/* The iterative-solver caller of the SpMV: CG for a symmetric positive
+ * definite matrix planned in FP32 or FP64 (any format / scheme).  One
+ * iteration (the plan's SpMV + four vector kernels, scalars kept on the
+ * device) is captured once as a CUDA graph and replayed; the residual is read
+ * every check_every iterations.  d_b, d_x: device vectors of n elements;
+ * d_x holds the start on entry and the solution on return.  Stops at
+ * ||b - A x|| / ||b|| <= rel_tol or after max_iters.  Deterministic.  The
+ * plan must outlive the solver; a plan is used by one solve at a time. */
+typedef struct sparsep_cg sparsep_cg;
+int sparsep_cg_create(sparsep_plan *plan, sparsep_cg **out);
+int sparsep_cg_solve(sparsep_cg *cg, const void *d_b, void *d_x, uint32_t max_iters, double rel_tol,
+                     uint32_t check_every, uint32_t *iters, double *rel_residual, void *stream);
+void sparsep_cg_free(sparsep_cg *cg);
+
+/* ------------------------------------------------------------------------ */
 /* Learned variant selector (no reference counterpart)                       */
 /* ------------------------------------------------------------------------ */
 /* Sixteen cheap sparsity features of a CSR structure with k right-hand sides

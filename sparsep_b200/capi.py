@@ -632,3 +632,41 @@ class Selector:
             self.free()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# conjugate gradient on a plan
+# ---------------------------------------------------------------------------
+class CG:
+    """Conjugate gradient (sparsep_cg_*) on an FP32 / FP64 plan of an SPD matrix."""
+
+    def __init__(self, plan: "Plan"):
+        L = lib()
+        L.sparsep_cg_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        L.sparsep_cg_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32,
+                                       C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.c_void_p]
+        L.sparsep_cg_free.argtypes = [C.c_void_p]
+        L.sparsep_cg_free.restype = None
+        self.plan = plan
+        h = C.c_void_p()
+        check(L.sparsep_cg_create(plan.h, C.byref(h)), "cg_create")
+        self.h = h
+
+    def solve(self, d_b: int, d_x: int, max_iters: int = 1000, rel_tol: float = 1e-8, check_every: int = 10,
+              stream: int | None = None):
+        """Solve in place on device vectors; returns (iterations, relative residual)."""
+        it, r = C.c_uint32(), C.c_double()
+        check(lib().sparsep_cg_solve(self.h, C.c_void_p(d_b), C.c_void_p(d_x), max_iters, rel_tol, check_every,
+                                     C.byref(it), C.byref(r), C.c_void_p(stream) if stream else None), "cg_solve")
+        return it.value, r.value
+
+    def free(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().sparsep_cg_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
