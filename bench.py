@@ -143,6 +143,24 @@ class Clocks:
                 "source": "nvml"}
 
 
+def max_over_ranks(v: float, world: int, device: str) -> float:
+    """The largest of every rank's v (the slowest rank times the job)."""
+    if world <= 1:
+        return float(v)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(bytes_per_step: int, steps: int, slowest_ms: float, world: int) -> float:
+    """GB/s of the whole job: every rank (replica) moves bytes_per_step per
+    step, and the job lasts as long as its slowest rank."""
+    return world * bytes_per_step * steps / (slowest_ms * 1e-3) / 1e9
+
+
 def run_ours(args, rank, world):
     import torch
     import torch.distributed as dist
@@ -190,14 +208,10 @@ def run_ours(args, rank, world):
     if world > 1:
         dist.barrier()
     ms = [a.elapsed_time(b) for a, b in evs]
-    tot_ms = sum(ms)
-    if world > 1:
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = max_over_ranks(sum(ms), world, "cuda")
     avg_ms = tot_ms / args.steps
     gbs_rank = cb / (avg_ms * 1e-3) / 1e9
-    value = world * cb * args.steps / (tot_ms * 1e-3) / 1e9
+    value = whole_job_gbs(cb, args.steps, tot_ms, world)
 
     # e2e through the C-ABI host path (pinned buffers, H2D x and D2H y per step)
     hx = torch.from_numpy(x).pin_memory()
@@ -213,11 +227,7 @@ def run_ours(args, rank, world):
         sp.capi.check(lib.sparsep_execute_host(plan.h, C.c_void_p(hx.data_ptr()), C.c_void_p(hy.data_ptr())))
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     phases = plan.timings()
-    e2e_avg = sum(e2e_ms) / len(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_avg], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_avg = float(t.item())
+    e2e_avg = max_over_ranks(sum(e2e_ms) / len(e2e_ms), world, "cuda")
     y_dev = yd.cpu().numpy()
     assert np.array_equal(y_dev, hy.numpy()), "device and host paths disagree"
 
