@@ -87,3 +87,31 @@ def test_batch_rejects_bad_variants():
     bad = sp.capi.BatchVariant(1, 3, 2048, 0)  # lanes not a power of two
     with pytest.raises(sp.SparsepError):
         b.set_variant(0, bad)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "i32"])
+def test_batch_wide_rhs(dtype):
+    """k = 64, 128, 256 right-hand sides (SpMM-like), default and applicable
+    candidate variants, every column against the oracle."""
+    rng = np.random.default_rng(8)
+    data = []
+    for m, k in enumerate((64, 128, 256)):
+        n = int(rng.integers(500, 1500))
+        rp, ci, vv = sp.synth.batch_matrix(rng, n, ("uniform", "zipf", "banded")[m], capi.DTYPES[dtype].np)
+        x = (rng.uniform(-1, 1, (n, k)) if dtype == "f32" else rng.integers(-8, 9, (n, k))).astype(
+            capi.DTYPES[dtype].np)
+        data.append((n, rp, ci, vv, k, x))
+    mats = [sp.csr(dtype, n, n, rp, ci, vv) for (n, rp, ci, vv, k, x) in data]
+    b = sp.capi.Batch(dtype, mats, [d[4] for d in data])
+    for m, d in enumerate(data):
+        b.set_x(m, d[5])
+    b.execute()
+    check_batch(b, mats, data, dtype)
+    for v in sp.capi.batch_candidates():
+        if not all(v.applies(d[4]) for d in data):
+            continue
+        for m in range(len(data)):
+            b.set_variant(m, v)
+        b.commit()
+        b.execute()
+        check_batch(b, mats, data, dtype)
