@@ -107,3 +107,13 @@ def test_compat_header_builds_reference_style_code(tmp_path, macro):
                         str(ROOT / "tests" / "compat_check.c"), f"-L{ROOT / 'sparsep_b200'}", "-lsparsep_b200",
                         "-o", str(out)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_api_example_builds(tmp_path):
+    """A C caller of the batch, selector, CG and value-reader entry points
+    (tests/api_example.c) compiles warning-free and links to the library."""
+    out = tmp_path / "api_example"
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", f"-I{ROOT / 'include'}",
+                        str(ROOT / "tests" / "api_example.c"), f"-L{ROOT / 'sparsep_b200'}", "-lsparsep_b200",
+                        "-o", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
