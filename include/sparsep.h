@@ -550,6 +550,25 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
 
 /* ------------------------------------------------------------------------ */
+/* COO -> CSR on the device (no reference counterpart on the device; the     */
+/* arrays equal coo2csr's, spmv/1D/CSR-row/support/matrix.h:113-152)         */
+/* ------------------------------------------------------------------------ */
+/* d_rows / d_cols / d_vals: nnz device entries in any order; d_rowptr:
+ * nrows + 1, d_colind / d_vals_out: nnz.  Rows ascending, input order kept
+ * inside a row (stable).  EINVAL if a row index is >= nrows.  Allocates its
+ * own scratch (16 bytes per nonzero); synchronises the stream. */
+#define SPARSEP_DECLARE_C2C(T, S)                                                                               \
+  int sparsep_coo2csr_device_##S(const uint32_t *d_rows, const uint32_t *d_cols, const T *d_vals, uint32_t nnz, \
+                                 uint32_t nrows, uint32_t *d_rowptr, uint32_t *d_colind, T *d_vals_out,         \
+                                 void *stream);
+SPARSEP_DECLARE_C2C(int8_t, i8)
+SPARSEP_DECLARE_C2C(int16_t, i16)
+SPARSEP_DECLARE_C2C(int32_t, i32)
+SPARSEP_DECLARE_C2C(int64_t, i64)
+SPARSEP_DECLARE_C2C(float, f32)
+SPARSEP_DECLARE_C2C(double, f64)
+
+/* ------------------------------------------------------------------------ */
 /* Conjugate gradient on a plan (no reference counterpart)                   */
 /* ------------------------------------------------------------------------ */
 /* The iterative-solver caller of the SpMV: CG for a symmetric positive
