@@ -567,6 +567,19 @@ SPARSEP_DECLARE_C2C(int32_t, i32)
 SPARSEP_DECLARE_C2C(int64_t, i64)
 SPARSEP_DECLARE_C2C(float, f32)
 SPARSEP_DECLARE_C2C(double, f64)
+/* A plan from a CSR matrix already on the device (e.g. the output above):
+ * the row pointers are read back for the planner, the column indices checked
+ * on the device, the arrays copied into the plan (the caller keeps its own). */
+#define SPARSEP_DECLARE_PLAN_DEVICE(T, S)                                                         \
+  int sparsep_plan_csr_device_##S(uint32_t nrows, uint32_t ncols, uint32_t nnz, const uint32_t *d_rowptr, \
+                                  const uint32_t *d_colind, const T *d_values, const sparsep_opts *o,     \
+                                  sparsep_plan **out);
+SPARSEP_DECLARE_PLAN_DEVICE(int8_t, i8)
+SPARSEP_DECLARE_PLAN_DEVICE(int16_t, i16)
+SPARSEP_DECLARE_PLAN_DEVICE(int32_t, i32)
+SPARSEP_DECLARE_PLAN_DEVICE(int64_t, i64)
+SPARSEP_DECLARE_PLAN_DEVICE(float, f32)
+SPARSEP_DECLARE_PLAN_DEVICE(double, f64)
 
 /* ------------------------------------------------------------------------ */
 /* Conjugate gradient on a plan (no reference counterpart)                   */

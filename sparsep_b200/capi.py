@@ -343,6 +343,24 @@ class Plan:
         self.info = PlanInfo()
         check(lib().sparsep_plan_get_info(self.h, C.byref(self.info)))
 
+    @classmethod
+    def from_device_csr(cls, dtype: str, nrows: int, ncols: int, nnz: int, d_rowptr: int, d_colind: int,
+                        d_values: int, opts: Opts | None = None) -> "Plan":
+        """A plan from CSR arrays already on the device (sparsep_plan_csr_device_*)."""
+        p = cls.__new__(cls)
+        p.A = None
+        p.dt = DTYPES[dtype]
+        h = C.c_void_p()
+        o = opts if opts is not None else default_opts()
+        f = getattr(lib(), f"sparsep_plan_csr_device_{dtype}")
+        f.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_void_p]
+        check(f(nrows, ncols, nnz, d_rowptr, d_colind, d_values, C.byref(o), C.byref(h)), f"plan_csr_device_{dtype}")
+        p.h = h
+        p.info = PlanInfo()
+        check(lib().sparsep_plan_get_info(p.h, C.byref(p.info)))
+        return p
+
     @property
     def nrows(self) -> int:
         return int(self.info.nrows)

@@ -106,7 +106,7 @@ static int upload(sparsep_plan *p, const void *h, size_t n, size_t es, size_t pa
   void *d = nullptr;
   int st = dalloc(p, (n + pad) * es, &d);
   if (st) return st;
-  if (n && h) CK(cudaMemcpyAsync(d, h, n * es, cudaMemcpyHostToDevice, p->stream));
+  if (n && h) CK(cudaMemcpyAsync(d, h, n * es, cudaMemcpyDefault, p->stream));  // host or device source
   p->info.device_bytes += (n + pad) * es;
   *out = d;
   return SPARSEP_OK;
@@ -407,7 +407,8 @@ static void set_out_mode(sparsep_plan *p, const sparsep_opts &o, uint32_t V, boo
 // CSR
 // ---------------------------------------------------------------------------
 template <typename T>
-static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, sparsep_plan **out) {
+static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, sparsep_plan **out,
+                    bool device_arrays = false) {
   sparsep_plan *p = nullptr;
   sparsep_opts oo;
   int st = begin_plan(out, Types<T>::dtype, SPARSEP_FMT_CSR, SPARSEP_1D, o, &p, oo);
@@ -418,8 +419,9 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
   if (A->rowptr[0] != 0 || A->rowptr[A->nrows] != A->nnz) return SPARSEP_EINVAL;
   for (uint32_t r = 0; r < A->nrows; ++r)
     if (A->rowptr[r + 1] < A->rowptr[r]) return SPARSEP_EINVAL;
-  for (uint32_t k = 0; k < A->nnz; ++k)
-    if (A->colind[k] >= A->ncols) return SPARSEP_EINVAL;
+  if (!device_arrays)  // device column indices are checked on the device by the caller
+    for (uint32_t k = 0; k < A->nnz; ++k)
+      if (A->colind[k] >= A->ncols) return SPARSEP_EINVAL;
   p->nrows = A->nrows;
   p->ncols = A->ncols;
   p->nnz = A->nnz;
@@ -1267,6 +1269,50 @@ static int check_err(sparsep_plan *p) {
   return SPARSEP_OK;
 }
 
+// Columns of a device CSR inside [0, ncols): one flag for the whole array.
+__global__ void cols_in_range(const uint32_t *__restrict__ c, uint64_t n, uint32_t ncols, int *__restrict__ bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (c[i] >= ncols) *bad = 1;
+}
+
+// A plan from a CSR matrix already on the device: the row pointers are read
+// back for the planner (4 bytes per row), the column indices are checked on
+// the device, and the arrays are copied device to device into the plan.
+template <typename T>
+static int plan_csr_device(uint32_t nrows, uint32_t ncols, uint32_t nnz, const uint32_t *d_rowptr,
+                           const uint32_t *d_colind, const T *d_values, const sparsep_opts *o, sparsep_plan **out) {
+  if (!out || !d_rowptr || (nnz && (!d_colind || !d_values))) return SPARSEP_EINVAL;
+  *out = nullptr;
+  std::vector<uint32_t> rp;
+  try {
+    rp.resize((size_t)nrows + 1);
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
+  }
+  CK(cudaMemcpy(rp.data(), d_rowptr, rp.size() * 4, cudaMemcpyDeviceToHost));
+  if (nnz) {
+    int *bad = nullptr, h = 0;
+    CK(cudaMalloc(&bad, sizeof(int)));
+    cudaError_t e = cudaMemset(bad, 0, sizeof(int));
+    if (e == cudaSuccess) {
+      cols_in_range<<<std::min<uint64_t>(4096, (nnz + 255) / 256), 256>>>(d_colind, nnz, ncols, bad);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h, bad, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    CK(e);
+    if (h) return SPARSEP_EINVAL;
+  }
+  typename Types<T>::csr A;
+  A.nrows = nrows;
+  A.ncols = ncols;
+  A.nnz = nnz;
+  A.rowptr = rp.data();
+  A.colind = const_cast<uint32_t *>(d_colind);
+  A.values = const_cast<T *>(d_values);
+  return plan_csr<T>(&A, o, out, true);
+}
+
 // ---------------------------------------------------------------------------
 // C-ABI
 // ---------------------------------------------------------------------------
@@ -1423,3 +1469,20 @@ SPARSEP_DTYPE_ENTRIES(float, f32)
 SPARSEP_DTYPE_ENTRIES(double, f64)
 
 }  // extern "C"
+
+#define SPARSEP_PLAN_DEVICE_ENTRY(T, S)                                                                   \
+  extern "C" int sparsep_plan_csr_device_##S(uint32_t nrows, uint32_t ncols, uint32_t nnz,                 \
+                                             const uint32_t *d_rowptr, const uint32_t *d_colind,          \
+                                             const T *d_values, const sparsep_opts *o, sparsep_plan **out) { \
+    try {                                                                                                 \
+      return plan_csr_device<T>(nrows, ncols, nnz, d_rowptr, d_colind, d_values, o, out);                 \
+    } catch (const std::bad_alloc &) {                                                                    \
+      return SPARSEP_ENOMEM;                                                                              \
+    }                                                                                                     \
+  }
+SPARSEP_PLAN_DEVICE_ENTRY(int8_t, i8)
+SPARSEP_PLAN_DEVICE_ENTRY(int16_t, i16)
+SPARSEP_PLAN_DEVICE_ENTRY(int32_t, i32)
+SPARSEP_PLAN_DEVICE_ENTRY(int64_t, i64)
+SPARSEP_PLAN_DEVICE_ENTRY(float, f32)
+SPARSEP_PLAN_DEVICE_ENTRY(double, f64)
