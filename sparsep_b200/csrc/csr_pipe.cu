@@ -17,6 +17,7 @@
 // planner sizes items so each fits one stage (<= CAP nonzeros, <= RCAP rows).
 // Waits are bounded: one that runs out records SPARSEP_ETIMEDOUT, and the CTA
 // waits (bounded) for its copies in flight before it returns.
+#include <atomic>
 #include "device.cuh"
 #include "kernels.hpp"
 
@@ -287,14 +288,19 @@ static cudaError_t launch_cap(const Params<T> &P, int sms, cudaStream_t st, int 
   constexpr int S = pipe_stages<T>();
   auto k = pipe::csr_pipe<T, S, CAP>;
   const size_t smem = pipe::Layout<T, CAP>::bytes(S);
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the shared-memory attribute, set once per device (concurrent host threads allowed)
+  static std::atomic<unsigned long long> set_on{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(set_on.load() & bit)) {
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    configured = true;
+    set_on.fetch_or(bit);
   }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, pipe::NT, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, pipe::NT, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   uint64_t grid = (uint64_t)sms * per_sm;

@@ -1,4 +1,6 @@
 // kernels.cu -- host launchers of the sm_100a SpMV kernels (kernels_impl.cuh).
+#include <atomic>
+
 #include "kernels_impl.cuh"
 #include "kernels.hpp"
 
@@ -10,12 +12,22 @@ namespace sparsep {
 template <typename T, int FMT, int RB, int CB>
 static cudaError_t launch_t(const Params<T> &P, uint32_t carry_w, int threads, size_t smem, cudaStream_t st) {
   auto k = spmv_items<T, FMT, RB, CB>;
-  // the default dynamic limit is 48 KB minus the kernel's static shared memory
-  static int configured = 0;
-  if (smem > 0 && (int)smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the default dynamic limit is 48 KB minus the kernel's static shared
+  // memory; the largest size set so far is kept per device (host threads may
+  // plan concurrently, on different devices)
+  static std::atomic<int> configured[64];
+  if (smem > 0) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    configured = (int)smem;
+    std::atomic<int> &c = configured[dev & 63];
+    if ((int)smem > c.load()) {
+      e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      int cur = c.load();
+      while ((int)smem > cur && !c.compare_exchange_weak(cur, (int)smem)) {
+      }
+    }
   }
   k<<<P.nitems, threads, smem, st>>>(P, carry_w);
   return cudaGetLastError();

@@ -202,3 +202,30 @@ def test_one_shot_and_device_paths():
     assert np.array_equal(y1, yd.cpu().numpy())  # same plan layout -> same order -> identical
     t = plan.timings()
     assert len(t) == 5 and t[0] > 0
+
+
+def test_concurrent_plans_from_host_threads():
+    """Plans built and executed from four host threads at once (x-staged 2D
+    tiles and the TMA pipeline set kernel attributes on first use): every
+    result equals the oracle."""
+    import concurrent.futures as cf
+
+    def one(i):
+        dtype = ("i32", "f32", "i64", "f64")[i % 4]
+        nrows, ncols, trip, x = make(dtype, seed=40 + i, nrows=2500 + 100 * i, ncols=2300, density=0.005)
+        r, c, v = trip
+        A = sp.cooe(dtype, nrows, ncols, r, c, v)
+        out = []
+        for M, o in ((sp.convert("cooe2dcsr", A, 4, 3), {}),
+                     (sp.csr(dtype, nrows, ncols, *sp.synth.to_csr(nrows, r, c, v)), dict(pipeline=1))):
+            out.append((dtype, sp.Plan(M, sp.default_opts(**o)).run_host(x), oracle_spmv(M, x), trip, x, nrows))
+        return out
+
+    with cf.ThreadPoolExecutor(4) as ex:
+        results = [r for rs in ex.map(one, range(8)) for r in rs]
+    for dtype, y, yo, (r, c, v), x, nrows in results:
+        if np.dtype(capi.DTYPES[dtype].np).kind != "f":
+            assert np.array_equal(y, yo)
+        else:
+            y_hi, a, cnt = hi_ref(r, c, v.astype(np.float64), x.astype(np.float64), nrows)
+            assert fp_bound_ok(y, y_hi, a, cnt, dtype)[0]
