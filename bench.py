@@ -231,6 +231,25 @@ def run_ours(args, rank, world):
     y_dev = yd.cpu().numpy()
     assert np.array_equal(y_dev, hy.numpy()), "device and host paths disagree"
 
+    # the gather floor: x read at this matrix's column indices and nothing else
+    ci_d = torch.from_numpy(colind[:nnz].view(np.int32)).cuda()
+    probe_out = torch.empty(592 * 512, dtype=torch.float32, device="cuda")
+    L = sp.lib()
+    L.sparsep_probe_gather_f32.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    g_ms = []
+    for i in range(args.warmup + 10):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sp.capi.check(L.sparsep_probe_gather_f32(ci_d.data_ptr(), nnz, xd.data_ptr(), probe_out.data_ptr(), 592,
+                                                 C.c_void_p(sh)), "probe_gather")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            g_ms.append(e0.elapsed_time(e1))
+    gather_floor_ms = statistics.median(g_ms)
+    del ci_d, probe_out
+
     peak, peak_kind = peaks()
     traffic = None
     tf = ROOT / "profiles" / "csr_f32_zipf1m_traffic.json"
@@ -246,7 +265,12 @@ def run_ours(args, rank, world):
                    "compulsory_bytes_per_step": cb, "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(gbs_rank, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(gbs_rank / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": cb, "avg_launch_ms": round(avg_ms, 5)},
+                     "algorithmic_bytes_per_launch": cb, "avg_launch_ms": round(avg_ms, 5),
+                     "gather_floor_ms": round(gather_floor_ms, 5),
+                     "frac_of_gather_floor": round(gather_floor_ms / avg_ms, 4),
+                     "gather_floor_note": "x read at this matrix's 16.7 M column indices and nothing else "
+                                          "(sparsep_probe_gather_f32, 592 x 512 threads, L2 flushed): the "
+                                          "random-gather bound of this SpMV"},
         "e2e": {"value": round(cb / (e2e_avg * 1e-3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": m * 4,
                 "d2h_bytes_per_step": n * 4, "ms_per_step": round(e2e_avg, 4),
                 "phases_ms": {"load_input_vector": phases[1], "kernel": phases[2],

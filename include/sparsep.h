@@ -582,6 +582,16 @@ SPARSEP_DECLARE_PLAN_DEVICE(float, f32)
 SPARSEP_DECLARE_PLAN_DEVICE(double, f64)
 
 /* ------------------------------------------------------------------------ */
+/* Gather floor (measurement support; no reference counterpart)              */
+/* ------------------------------------------------------------------------ */
+/* Reads x[d_idx[i]] for i < n (column indices all < length of x) and
+ * nothing else, on `ctas` CTAs of 512 threads; d_out receives one float per
+ * thread (ctas * 512).  Timing it on a matrix's column indices gives the
+ * random-gather bound of that matrix's SpMV. */
+int sparsep_probe_gather_f32(const uint32_t *d_idx, uint64_t n, const float *d_x, float *d_out, int ctas,
+                             void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Conjugate gradient on a plan (no reference counterpart)                   */
 /* ------------------------------------------------------------------------ */
 /* The iterative-solver caller of the SpMV: CG for a symmetric positive
