@@ -346,6 +346,8 @@ typedef struct sparsep_plan_info {
   int32_t kernel_launches; /* kernels launched per execution                   */
   int32_t lanes, workers, stage_x;
   char variant[96];       /* human-readable variant name                      */
+  int32_t y_bands;        /* host-buffer path: row bands of y copied back while
+                             the kernel runs (0: one copy after the kernel)     */
 } sparsep_plan_info;
 
 int sparsep_plan_get_info(const sparsep_plan *plan, sparsep_plan_info *info);
@@ -358,7 +360,10 @@ void sparsep_plan_free(sparsep_plan *plan);
 int sparsep_execute_device(sparsep_plan *plan, const void *d_x, void *d_y, void *stream);
 
 /* Execute with HOST pointers: H2D x, kernel(s), D2H y, synchronous.  Fills the
- * timer slots 1..4. */
+ * timer slots 1..4.  1D CSR plans with at least 1 MB of y copy y back in up to
+ * 8 row bands (info.y_bands), each as soon as the kernel has finished the
+ * items writing it; slot 3 is then the part of the copy left after the
+ * kernel.  A pinned y buffer lets the band copies run without host waits. */
 int sparsep_execute_host(sparsep_plan *plan, const void *h_x, void *h_y);
 
 /* Device-resident x / y buffers owned by the plan (ncols*nrhs, nrows*nrhs). */

@@ -65,7 +65,8 @@ class PlanInfo(C.Structure):
                 ("nrows", C.c_uint32), ("ncols", C.c_uint32), ("nnz", C.c_uint64), ("nblocks", C.c_uint64),
                 ("items", C.c_uint64), ("tiles", C.c_uint64), ("compulsory_bytes", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("scratch_bytes", C.c_uint64), ("kernel_launches", C.c_int32),
-                ("lanes", C.c_int32), ("workers", C.c_int32), ("stage_x", C.c_int32), ("variant", C.c_char * 96)]
+                ("lanes", C.c_int32), ("workers", C.c_int32), ("stage_x", C.c_int32), ("variant", C.c_char * 96),
+                ("y_bands", C.c_int32)]
 
 
 def _struct_types(dt: DType) -> dict[str, type]:

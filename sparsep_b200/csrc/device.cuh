@@ -145,6 +145,7 @@ struct Item {
   uint32_t nchunk;      // ITEM_LONG: chunks of the row
   uint32_t first;       // ITEM_LONG: item index of the row's chunk 0
   uint32_t cslot;       // ITEM_LONG: the row's arrival counter
+  uint32_t band;        // row band of y the item writes (host-buffer path, see Params::band_cnt)
 };
 
 // Per-launch parameters shared by all kernels.
@@ -174,6 +175,7 @@ template <typename T> struct Params {
   unsigned long long *carry_idx;  // output index or ~0ull
   unsigned int *done;             // completion counter, reset by the last CTA
   unsigned int *row_cnt;          // per long row arrival counters (pipelined CSR)
+  unsigned int *band_cnt;         // when set: items finished per row band of y (one counter per band)
   int *err;                       // device error word (bounded waits, checked builds)
   // array extents, used by the bounds-checked build (-DSPARSEP_CHECK)
   uint64_t n_rowptr, n_idx, n_val, n_elems, n_x, n_xalloc, n_carry;

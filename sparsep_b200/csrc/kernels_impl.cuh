@@ -727,6 +727,15 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
       if (threadIdx.x == 0) *P.done = 0;
     }
   }
+
+  // Host-buffer path: the item is counted in its row band once all of its
+  // writes to y are visible device-wide; a copy stream waiting on the band's
+  // count moves those rows to the host while later items still run.
+  if (P.band_cnt != nullptr) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(P.band_cnt + it.band, 1u);
+  }
 }
 
 // ---------------------------------------------------------------------------

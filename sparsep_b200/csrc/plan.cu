@@ -9,6 +9,7 @@
 // reference split exactly (one part = one CTA, one tasklet = one warp) and
 // nr_parts = 0 lets the planner size items for the GPU.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -19,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "internal.hpp"
 #include "kernels.hpp"
 
@@ -27,6 +30,10 @@ using namespace sparsep;
 // ---------------------------------------------------------------------------
 // plan object
 // ---------------------------------------------------------------------------
+// Row bands of y for the host-buffer path (each >= BAND_MIN_BYTES of y).
+static constexpr uint32_t MAX_BANDS = 8;
+static constexpr size_t BAND_MIN_BYTES = 512 * 1024;
+
 struct sparsep_plan {
   int dtype = 0, format = 0, scheme = 0, nrhs = 1;
   size_t esize = 4;
@@ -47,6 +54,15 @@ struct sparsep_plan {
   unsigned long long *carry_val = nullptr, *carry_idx = nullptr;
   unsigned int *done = nullptr;
   int *err = nullptr;
+  int *h_err = nullptr;  // pinned host copy of the error word (host-buffer path)
+  // Host-buffer path: y goes back in row bands, each copied as soon as the
+  // kernel has finished the items writing it (nbands = 0: one copy at the end).
+  uint32_t nbands = 0;
+  uint32_t band_row[MAX_BANDS + 1] = {};  // band b = rows [band_row[b], band_row[b+1])
+  uint32_t band_items[MAX_BANDS] = {};    // items of band b: the count its copy waits for
+  unsigned int *band_cnt = nullptr;       // device counters, cleared before each launch
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t band_ev = nullptr;          // counters cleared (on the plan's stream)
   unsigned int *row_cnt = nullptr;  // long-row arrival counters (pipelined CSR)
   uint64_t n_rowptr = 0, n_idx = 0, n_val = 0, n_elems = 0;  // allocated extents
   bool stage = false;
@@ -273,10 +289,75 @@ static std::vector<uint64_t> even_cuts(uint64_t e0, uint64_t e1, uint64_t per) {
 }
 
 // ---------------------------------------------------------------------------
+// Row bands of the host-buffer path
+// ---------------------------------------------------------------------------
+// cuStreamWaitValue32 from the driver, looked up through the runtime (the
+// library does not link libcuda); null when the driver does not offer it.
+using WaitValue32 = CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int);
+static WaitValue32 wait_value32() {
+  static const WaitValue32 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuStreamWaitValue32", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<WaitValue32>(f);
+  }();
+  return fn;
+}
+
+// Splits a 1D CSR item list into up to MAX_BANDS row bands of y: contiguous
+// item ranges whose written rows (row items [a0, a1), long-row chunks their
+// row) are disjoint and ordered.  A cut before item i is valid when no earlier
+// item writes a row at or past the first row written by item i or any later
+// item.  Sets each item's band and the plan's band rows / item counts.
+static void set_bands(sparsep_plan *p, std::vector<Item> &items) {
+  p->nbands = 0;
+  const size_t ybytes = (size_t)p->nrows * p->esize, n = items.size();
+  if (p->format != SPARSEP_FMT_CSR || p->scheme != SPARSEP_1D || p->out_mode != OUT_DIRECT || p->pipe || n < 2 ||
+      ybytes < 2 * BAND_MIN_BYTES || !wait_value32())
+    return;
+  std::vector<uint64_t> pm(n), sm(n);  // prefix max of row ends, suffix min of row starts
+  for (size_t i = 0; i < n; ++i) {
+    const Item &it = items[i];
+    uint64_t hi;
+    if (it.kind == ITEM_ROWS) {
+      sm[i] = (uint64_t)it.row_off + it.a0;
+      hi = (uint64_t)it.row_off + it.a1;
+    } else if (it.kind == ITEM_LONG) {
+      sm[i] = it.crow;
+      hi = (uint64_t)it.crow + 1;
+    } else {
+      return;
+    }
+    pm[i] = std::max(hi, i ? pm[i - 1] : 0);
+  }
+  for (size_t i = n - 1; i-- > 0;) sm[i] = std::min(sm[i], sm[i + 1]);
+  const uint32_t want = (uint32_t)std::min<size_t>(MAX_BANDS, ybytes / BAND_MIN_BYTES);
+  std::vector<size_t> cut{0};
+  for (uint32_t k = 1; k < want; ++k) {
+    size_t i = std::max(cut.back() + 1, (size_t)k * n / want);
+    while (i < n && pm[i - 1] > sm[i]) ++i;
+    if (i >= n) break;
+    cut.push_back(i);
+  }
+  if (cut.size() < 2) return;
+  cut.push_back(n);
+  p->nbands = (uint32_t)cut.size() - 1;
+  p->band_row[0] = 0;
+  for (uint32_t b = 0; b < p->nbands; ++b) {
+    p->band_items[b] = (uint32_t)(cut[b + 1] - cut[b]);
+    for (size_t i = cut[b]; i < cut[b + 1]; ++i) items[i].band = b;
+    p->band_row[b + 1] = b + 1 < p->nbands ? (uint32_t)sm[cut[b + 1]] : p->nrows;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Plan finalisation
 // ---------------------------------------------------------------------------
 static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_opts &o) {
   p->nitems = (uint32_t)items.size();
+  set_bands(p, items);
   int st = upload(p, items.data(), items.size(), sizeof(Item), 0, (const void **)&p->items);
   if (st) return st;
   // x with >= 16 bytes of zero slack (bulk-copy alignment), y, partial slices
@@ -302,6 +383,13 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   }
   st = dalloc(p, 16, (void **)&p->err);
   if (st) return st;
+  CK(cudaHostAlloc((void **)&p->h_err, sizeof(int), cudaHostAllocDefault));
+  if (p->nbands) {
+    st = dalloc(p, MAX_BANDS * sizeof(unsigned int), (void **)&p->band_cnt);
+    if (st) return st;
+    CK(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&p->band_ev, cudaEventDisableTiming));
+  }
   uint32_t nlong = 0;
   for (const Item &it : items) nlong += it.kind == ITEM_LONG && it.chunk == 0;
   if (nlong) {
@@ -334,6 +422,7 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   p->info.kernel_launches = 1 + (p->out_mode == OUT_PARTIAL ? 1 : 0);
   p->info.workers = workers;
   p->info.stage_x = p->stage ? 1 : 0;
+  p->info.y_bands = (int32_t)p->nbands;
   int lanes_min = 64, lanes_max = -1;  // over row items; 0 = staged stream kernel
   for (const Item &it : items)
     if (it.kind == ITEM_ROWS) {
@@ -1192,7 +1281,7 @@ static int plan_bdbcoo(const typename Types<T>::bdbcoo *A, const sparsep_opts *o
 // Execution
 // ---------------------------------------------------------------------------
 template <typename T>
-static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
+static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s, unsigned int *band_cnt) {
   const T *x = static_cast<const T *>(d_x);
   if (p->stage && d_x != p->xpad) {
     CK(cudaMemcpyAsync(p->xpad, d_x, (size_t)p->ncols * sizeof(T), cudaMemcpyDeviceToDevice, s));
@@ -1224,6 +1313,7 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   P.carry_idx = (p->carry_w && p->format != SPARSEP_FMT_CSR) ? p->carry_idx : nullptr;
   P.done = p->done;
   P.row_cnt = p->row_cnt;
+  P.band_cnt = band_cnt;
   P.err = p->err;
   P.n_rowptr = p->n_rowptr;
   P.n_idx = p->n_idx;
@@ -1243,30 +1333,17 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
   return SPARSEP_OK;
 }
 
-static int run_any(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
+static int run_any(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s,
+                   unsigned int *band_cnt = nullptr) {
   switch (p->dtype) {
-    case SPARSEP_INT8: return run_t<int8_t>(p, d_x, d_y, s);
-    case SPARSEP_INT16: return run_t<int16_t>(p, d_x, d_y, s);
-    case SPARSEP_INT32: return run_t<int32_t>(p, d_x, d_y, s);
-    case SPARSEP_INT64: return run_t<int64_t>(p, d_x, d_y, s);
-    case SPARSEP_FP32: return run_t<float>(p, d_x, d_y, s);
-    case SPARSEP_FP64: return run_t<double>(p, d_x, d_y, s);
+    case SPARSEP_INT8: return run_t<int8_t>(p, d_x, d_y, s, band_cnt);
+    case SPARSEP_INT16: return run_t<int16_t>(p, d_x, d_y, s, band_cnt);
+    case SPARSEP_INT32: return run_t<int32_t>(p, d_x, d_y, s, band_cnt);
+    case SPARSEP_INT64: return run_t<int64_t>(p, d_x, d_y, s, band_cnt);
+    case SPARSEP_FP32: return run_t<float>(p, d_x, d_y, s, band_cnt);
+    case SPARSEP_FP64: return run_t<double>(p, d_x, d_y, s, band_cnt);
   }
   return SPARSEP_EINVAL;
-}
-
-// The error word after the plan's stream has drained; reset for the next run.
-static int check_err(sparsep_plan *p) {
-  int e = 0;
-  CK(cudaStreamSynchronize(p->stream));
-  CK(cudaMemcpyAsync(&e, p->err, sizeof e, cudaMemcpyDeviceToHost, p->stream));
-  CK(cudaStreamSynchronize(p->stream));
-  if (e) {
-    CK(cudaMemsetAsync(p->err, 0, sizeof e, p->stream));
-    CK(cudaStreamSynchronize(p->stream));
-    return e;
-  }
-  return SPARSEP_OK;
 }
 
 // Columns of a device CSR inside [0, ncols): one flag for the whole array.
@@ -1372,6 +1449,12 @@ void sparsep_plan_free(sparsep_plan *p) {
   if (!p) return;
   if (p->stream) cudaStreamSynchronize(p->stream);
   for (void *d : p->allocs) cudaFree(d);
+  if (p->h_err) cudaFreeHost(p->h_err);
+  if (p->copy_stream) {
+    cudaStreamSynchronize(p->copy_stream);
+    cudaStreamDestroy(p->copy_stream);
+  }
+  if (p->band_ev) cudaEventDestroy(p->band_ev);
   for (auto &e : p->ev)
     if (e) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -1398,18 +1481,55 @@ int sparsep_execute_device(sparsep_plan *p, const void *d_x, void *d_y, void *st
   return run_any(p, d_x, d_y, static_cast<cudaStream_t>(stream));
 }
 
+// y in row bands: each band's copy, on the plan's copy stream, waits
+// (cuStreamWaitValue32) until the kernel has counted all items of the band, so
+// the copies of the early bands overlap the kernel's later items.
+static int copy_y_banded(sparsep_plan *p, void *h_y) {
+  cudaStream_t c = p->copy_stream;
+  const size_t es = p->esize;
+  char *hy = static_cast<char *>(h_y);
+  const char *dy = static_cast<const char *>(p->y);
+  uint32_t b = 0;
+  for (; b < p->nbands; ++b) {
+    if (wait_value32()(c, (CUdeviceptr)(uintptr_t)(p->band_cnt + b), p->band_items[b], CU_STREAM_WAIT_VALUE_GEQ) !=
+        CUDA_SUCCESS)
+      break;
+    const size_t r0 = p->band_row[b], r1 = p->band_row[b + 1];
+    if (r1 > r0) CK(cudaMemcpyAsync(hy + r0 * es, dy + r0 * es, (r1 - r0) * es, cudaMemcpyDeviceToHost, c));
+  }
+  if (b < p->nbands) {  // the driver refused a wait: the remaining rows after the whole kernel
+    CK(cudaStreamWaitEvent(c, p->ev[2], 0));
+    const size_t r0 = p->band_row[b];
+    CK(cudaMemcpyAsync(hy + r0 * es, dy + r0 * es, (p->nrows - r0) * es, cudaMemcpyDeviceToHost, c));
+  }
+  return SPARSEP_OK;
+}
+
 int sparsep_execute_host(sparsep_plan *p, const void *h_x, void *h_y) {
   if (!p || !h_x || !h_y) return SPARSEP_EINVAL;
   cudaStream_t s = p->stream;
   CK(cudaEventRecord(p->ev[0], s));
   CK(cudaMemcpyAsync(p->xpad, h_x, (size_t)p->ncols * p->esize, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(p->ev[1], s));
-  int st = run_any(p, p->xpad, p->y, s);
-  if (st) return st;
-  if (p->out_mode != OUT_PARTIAL) CK(cudaEventRecord(p->ev[2], s));
-  CK(cudaEventRecord(p->ev[3], s));
-  CK(cudaMemcpyAsync(h_y, p->y, (size_t)p->nrows * p->esize, cudaMemcpyDeviceToHost, s));
-  CK(cudaEventRecord(p->ev[4], s));
+  if (p->nbands) {
+    CK(cudaMemsetAsync(p->band_cnt, 0, p->nbands * sizeof(unsigned int), s));
+    CK(cudaEventRecord(p->band_ev, s));
+    CK(cudaStreamWaitEvent(p->copy_stream, p->band_ev, 0));  // counters cleared before any wait reads them
+    if (int st = run_any(p, p->xpad, p->y, s, p->band_cnt)) return st;
+    CK(cudaEventRecord(p->ev[2], s));
+    CK(cudaEventRecord(p->ev[3], s));
+    if (int st = copy_y_banded(p, h_y)) return st;
+    CK(cudaEventRecord(p->ev[4], p->copy_stream));
+    CK(cudaStreamWaitEvent(s, p->ev[4], 0));
+  } else {
+    if (int st = run_any(p, p->xpad, p->y, s)) return st;
+    if (p->out_mode != OUT_PARTIAL) CK(cudaEventRecord(p->ev[2], s));
+    CK(cudaEventRecord(p->ev[3], s));
+    CK(cudaMemcpyAsync(h_y, p->y, (size_t)p->nrows * p->esize, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(p->ev[4], s));
+  }
+  // the error word rides behind y: one synchronisation for the whole call
+  CK(cudaMemcpyAsync(p->h_err, p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   float a = 0, b = 0, c = 0, d = 0;
   CK(cudaEventElapsedTime(&a, p->ev[0], p->ev[1]));
@@ -1419,8 +1539,13 @@ int sparsep_execute_host(sparsep_plan *p, const void *h_x, void *h_y) {
   p->t[1] = a;
   p->t[2] = b;
   p->t[4] = c;
-  p->t[3] = d;
-  return check_err(p);
+  p->t[3] = std::max(d, 0.f);  // banded: the part of the y copy left after the kernel
+  if (const int e = *p->h_err) {
+    CK(cudaMemsetAsync(p->err, 0, sizeof(int), s));
+    CK(cudaStreamSynchronize(s));
+    return e;
+  }
+  return SPARSEP_OK;
 }
 
 #define SPARSEP_KIND_ENTRIES(T, S, K)                                                                 \

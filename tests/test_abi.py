@@ -117,3 +117,21 @@ def test_api_example_builds(tmp_path):
                         str(ROOT / "tests" / "api_example.c"), f"-L{ROOT / 'sparsep_b200'}", "-lsparsep_b200",
                         "-o", str(out)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_plan_info_layout_matches_header(tmp_path):
+    """capi.PlanInfo mirrors sparsep_plan_info field for field (size and the
+    offsets of every field, from a C program compiled against the header)."""
+    names = [f[0] for f in capi.PlanInfo._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"sparsep.h\"\nint main(void) {\n"
+                   '  printf("%zu", sizeof(sparsep_plan_info));\n'
+                   + "".join(f'  printf(" %zu", offsetof(sparsep_plan_info, {n}));\n' for n in names)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(capi.PlanInfo)] + [getattr(capi.PlanInfo, n).offset for n in names]
+    assert got == want

@@ -45,7 +45,8 @@ def make(dtype, seed=0, nrows=3001, ncols=2903, density=0.004, long_row=11, empt
 OPTS_1D = [dict(), dict(sync=capi.SYNC_ATOMIC), dict(nr_parts=7, part_balance=capi.BAL_ROW),
            dict(nr_parts=64, part_balance=capi.BAL_NNZ, worker_balance=capi.BAL_NNZ),
            dict(nr_parts=33, part_balance=capi.BAL_NNZ_ELEM), dict(lanes=1), dict(lanes=32, nr_workers=4),
-           dict(pipeline=1), dict(pipeline=1, item_nnz=2048), dict(item_nnz=2048), dict(nr_workers=16)]
+           dict(pipeline=1), dict(pipeline=1, item_nnz=2048), dict(item_nnz=2048), dict(nr_workers=16),
+           dict(nr_workers=4)]
 
 
 @pytest.mark.parametrize("dtype", DT)
