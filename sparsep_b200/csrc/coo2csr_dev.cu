@@ -6,7 +6,7 @@
 // Stable LSD radix sort of (row, input index) pairs, 4 bits per pass, only as
 // many passes as the row count needs (20 bits -> 5 passes for 1M rows):
 //   hist     per 1024-element tile, counts of each digit  -> hist[d][tile]
-//   scan     exclusive scan of hist in digit-major order (one CTA)
+//   scan     exclusive scan of hist in digit-major order (three launches)
 //   scatter  each element to scan[d][tile] + (earlier elements of its tile
 //            with digit d): the tile is walked in four 256-element rounds;
 //            inside a round, __match_any_sync gives the rank among the warp's
@@ -47,28 +47,82 @@ __global__ void __launch_bounds__(NT) hist(const uint32_t *__restrict__ key, uin
   if (threadIdx.x < RADIX) h[(size_t)threadIdx.x * nt + blockIdx.x] = c[threadIdx.x];
 }
 
-// exclusive scan of m counts in place, one CTA, chunks of NT in order
-__global__ void __launch_bounds__(NT) scan(uint32_t *__restrict__ h, uint32_t m) {
-  __shared__ uint32_t s[NT];
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (uint32_t b = 0; b < m; b += NT) {
-    const uint32_t i = b + threadIdx.x;
-    const uint32_t v = i < m ? h[i] : 0;
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int o = 1; o < NT; o <<= 1) {  // inclusive Hillis-Steele scan
-      const uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
-      __syncthreads();
-      s[threadIdx.x] += t;
-      __syncthreads();
-    }
-    if (i < m) h[i] = carry + s[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == NT - 1) carry += s[NT - 1];
-    __syncthreads();
+// Exclusive scan of the m digit counts in place, in three launches:
+//   scan_reduce  CTA b sums its chunk h[b*SCAN_CHUNK, ...)        -> sums[b]
+//   scan_top     one CTA scans sums[0, nb) (exclusive), in chunks
+//   scan_down    CTA b scans its chunk and adds sums[b]
+// A chunk is SCAN_CHUNK = 4 counts per thread; a thread scans its 4 serially
+// and the CTA scans the thread totals with warp shuffles.
+constexpr int SCAN_CHUNK = 4 * NT;
+
+// exclusive scan of v over the CTA; *total gets the sum of all v
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t *total) {
+  __shared__ uint32_t ws[NT / 32 + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
   }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = lane < NT / 32 ? ws[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    if (lane < NT / 32) ws[lane] = wi - w;
+    if (lane == NT / 32 - 1) ws[NT / 32] = wi;
+  }
+  __syncthreads();
+  const uint32_t r = ws[warp] + inc - v;
+  *total = ws[NT / 32];
+  __syncthreads();  // ws is reused by the next call
+  return r;
+}
+
+// exclusive scan of a[base, base + SCAN_CHUNK) (clipped to m) plus offset; returns the chunk's sum
+__device__ __forceinline__ uint32_t scan_chunk(uint32_t *__restrict__ a, uint32_t m, uint32_t base, uint32_t offset) {
+  const uint32_t i0 = base + 4 * threadIdx.x;
+  uint32_t v[4], t = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = i0 + k < m ? a[i0 + k] : 0u;
+    t += v[k];
+  }
+  uint32_t total;
+  uint32_t run = offset + block_scan(t, &total);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (i0 + k < m) a[i0 + k] = run;
+    run += v[k];
+  }
+  return total;
+}
+
+__global__ void __launch_bounds__(NT) scan_reduce(const uint32_t *__restrict__ h, uint32_t m,
+                                                  uint32_t *__restrict__ sums) {
+  const uint32_t i0 = blockIdx.x * SCAN_CHUNK + 4 * threadIdx.x;
+  uint32_t t = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) t += i0 + k < m ? h[i0 + k] : 0u;
+  uint32_t total;
+  block_scan(t, &total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(NT) scan_top(uint32_t *__restrict__ sums, uint32_t nb) {
+  uint32_t carry = 0;
+  for (uint32_t b = 0; b < nb; b += SCAN_CHUNK) carry += scan_chunk(sums, nb, b, carry);
+}
+
+__global__ void __launch_bounds__(NT) scan_down(uint32_t *__restrict__ h, uint32_t m,
+                                                const uint32_t *__restrict__ sums) {
+  scan_chunk(h, m, blockIdx.x * SCAN_CHUNK, sums[blockIdx.x]);
 }
 
 __global__ void __launch_bounds__(NT) scatter(const uint32_t *__restrict__ key, const uint32_t *__restrict__ idx,
@@ -156,7 +210,8 @@ static int coo2csr_device(const uint32_t *rows, const uint32_t *cols, const void
   const uint32_t nt = (nnz + TILE - 1) / TILE;
   uint32_t *buf = nullptr;
   int *bad = nullptr;
-  const size_t words = 4 * (size_t)nnz + (size_t)RADIX * nt + 8;
+  const uint32_t m = RADIX * nt, nb = (m + SCAN_CHUNK - 1) / SCAN_CHUNK;  // digit counts, scan chunks
+  const size_t words = 4 * (size_t)nnz + (size_t)m + nb + 8;
   int st = c2c_err(cudaMalloc(&buf, words * 4));
   if (!st) st = c2c_err(cudaMalloc(&bad, sizeof(int)));
   if (st) {
@@ -164,14 +219,16 @@ static int coo2csr_device(const uint32_t *rows, const uint32_t *cols, const void
     cudaFree(bad);
     return st;
   }
-  uint32_t *k0 = buf, *i0 = k0 + nnz, *k1 = i0 + nnz, *i1 = k1 + nnz, *h = i1 + nnz;
+  uint32_t *k0 = buf, *i0 = k0 + nnz, *k1 = i0 + nnz, *i1 = k1 + nnz, *h = i1 + nnz, *sums = h + m;
   const uint32_t *key = rows, *idx = nullptr;
   int h_bad = 0;
   st = c2c_err(cudaMemsetAsync(bad, 0, sizeof(int), s));
   for (int shift = 0; !st && nnz && shift < (bits ? bits : 1); shift += 4) {
     uint32_t *ko = (shift / 4) % 2 ? k1 : k0, *io = (shift / 4) % 2 ? i1 : i0;
     hist<<<nt, NT, 0, s>>>(key, nnz, shift, nt, h, nrows, shift == 0 ? bad : nullptr);
-    scan<<<1, NT, 0, s>>>(h, RADIX * nt);
+    scan_reduce<<<nb, NT, 0, s>>>(h, m, sums);
+    scan_top<<<1, NT, 0, s>>>(sums, nb);
+    scan_down<<<nb, NT, 0, s>>>(h, m, sums);
     scatter<<<nt, NT, 0, s>>>(key, idx, nnz, shift, nt, h, ko, io);
     st = c2c_err(cudaGetLastError());
     key = ko;
