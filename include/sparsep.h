@@ -587,6 +587,49 @@ SPARSEP_DECLARE_PLAN_DEVICE(float, f32)
 SPARSEP_DECLARE_PLAN_DEVICE(double, f64)
 
 /* ------------------------------------------------------------------------ */
+/* CSR -> BCSR on the device (the arrays of sparsep_csr2bcsr_<t>:           */
+/* spmv/1D/BCSR-nnz/support/matrix.h:202-485, csr2bcsr + sortBCSRMatrix +   */
+/* countNNZperBlockBCSRMatrix)                                              */
+/* ------------------------------------------------------------------------ */
+/* Two steps.  sparsep_bcsr_layout_device sorts the nonzeros of a device CSR
+ * (rowptr nrows + 1, colind nnz) into rb x cb blocks and returns the block
+ * count; EINVAL for a malformed rowptr or a column >= ncols.  The fill then
+ * writes caller-allocated device arrays: browptr[ceil(nrows/rb) + 1],
+ * bcolind[nblocks], bval[nblocks * rb * cb] (row-major blocks, blocks of a
+ * block row by ascending block column, a later duplicate entry overwrites an
+ * earlier one) and nnz_per_block[nblocks] (entries != 0).  One layout serves
+ * any number of fills (e.g. several value arrays of one pattern) while the
+ * CSR's colind stays unchanged; both steps synchronise the stream. */
+typedef struct sparsep_bcsr_layout sparsep_bcsr_layout;
+int sparsep_bcsr_layout_device(const uint32_t *d_rowptr, const uint32_t *d_colind, uint32_t nrows, uint32_t ncols,
+                               uint32_t nnz, uint32_t rb, uint32_t cb, sparsep_bcsr_layout **out, uint64_t *nblocks,
+                               void *stream);
+void sparsep_bcsr_layout_free(sparsep_bcsr_layout *layout);
+#define SPARSEP_DECLARE_C2B(T, S)                                                                                \
+  int sparsep_csr2bcsr_device_##S(const sparsep_bcsr_layout *layout, const T *d_values, uint32_t *d_browptr, \
+                                  uint32_t *d_bcolind, T *d_bval, uint32_t *d_nnz_per_block, void *stream);
+SPARSEP_DECLARE_C2B(int8_t, i8)
+SPARSEP_DECLARE_C2B(int16_t, i16)
+SPARSEP_DECLARE_C2B(int32_t, i32)
+SPARSEP_DECLARE_C2B(int64_t, i64)
+SPARSEP_DECLARE_C2B(float, f32)
+SPARSEP_DECLARE_C2B(double, f64)
+/* A 1D BCSR plan from device arrays (the output above): browptr (and, for
+ * nnz-balanced parts, nnz_per_block, which may otherwise be NULL) read back
+ * for the planner, block columns checked on the device, arrays copied. */
+#define SPARSEP_DECLARE_PLAN_BCSR_DEVICE(T, S)                                                                   \
+  int sparsep_plan_bcsr_device_##S(uint32_t nrows, uint32_t ncols, uint32_t rb, uint32_t cb, uint64_t nblocks, \
+                                   uint64_t nnz, const uint32_t *d_browptr, const uint32_t *d_bcolind,         \
+                                   const T *d_bval, const uint32_t *d_nnz_per_block, const sparsep_opts *o,    \
+                                   sparsep_plan **out);
+SPARSEP_DECLARE_PLAN_BCSR_DEVICE(int8_t, i8)
+SPARSEP_DECLARE_PLAN_BCSR_DEVICE(int16_t, i16)
+SPARSEP_DECLARE_PLAN_BCSR_DEVICE(int32_t, i32)
+SPARSEP_DECLARE_PLAN_BCSR_DEVICE(int64_t, i64)
+SPARSEP_DECLARE_PLAN_BCSR_DEVICE(float, f32)
+SPARSEP_DECLARE_PLAN_BCSR_DEVICE(double, f64)
+
+/* ------------------------------------------------------------------------ */
 /* Gather floor (measurement support; no reference counterpart)              */
 /* ------------------------------------------------------------------------ */
 /* Reads x[d_idx[i]] for i < n (column indices all < length of x) and

@@ -362,6 +362,26 @@ class Plan:
         check(lib().sparsep_plan_get_info(p.h, C.byref(p.info)))
         return p
 
+    @classmethod
+    def from_device_bcsr(cls, dtype: str, nrows: int, ncols: int, rb: int, cb: int, nblocks: int, nnz: int,
+                         d_browptr: int, d_bcolind: int, d_bval: int, d_nnz_per_block: int | None,
+                         opts: Opts | None = None) -> "Plan":
+        """A 1D BCSR plan from arrays already on the device (sparsep_plan_bcsr_device_*)."""
+        p = cls.__new__(cls)
+        p.A = None
+        p.dt = DTYPES[dtype]
+        h = C.c_void_p()
+        o = opts if opts is not None else default_opts()
+        f = getattr(lib(), f"sparsep_plan_bcsr_device_{dtype}")
+        f.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
+                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        check(f(nrows, ncols, rb, cb, nblocks, nnz, d_browptr, d_bcolind, d_bval, d_nnz_per_block, C.byref(o),
+                C.byref(h)), f"plan_bcsr_device_{dtype}")
+        p.h = h
+        p.info = PlanInfo()
+        check(lib().sparsep_plan_get_info(p.h, C.byref(p.info)))
+        return p
+
     @property
     def nrows(self) -> int:
         return int(self.info.nrows)
@@ -397,6 +417,45 @@ class Plan:
     def free(self) -> None:
         if getattr(self, "h", None) and self.h.value:
             lib().sparsep_plan_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class BcsrLayout:
+    """The block structure of a device CSR (sparsep_bcsr_layout_device): sorts
+    the nonzeros into rb x cb blocks once; fill() then writes the BCSR arrays
+    of one value array into caller-allocated device buffers."""
+
+    def __init__(self, d_rowptr: int, d_colind: int, nrows: int, ncols: int, nnz: int, rb: int, cb: int,
+                 stream: int = 0):
+        L = lib()
+        L.sparsep_bcsr_layout_device.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                 C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.sparsep_bcsr_layout_free.argtypes = [C.c_void_p]
+        L.sparsep_bcsr_layout_free.restype = None
+        self.h = C.c_void_p()
+        nb = C.c_uint64()
+        check(L.sparsep_bcsr_layout_device(d_rowptr, d_colind, nrows, ncols, nnz, rb, cb, C.byref(self.h),
+                                           C.byref(nb), C.c_void_p(stream)), "bcsr_layout_device")
+        self.nblocks = int(nb.value)
+        self.nrows, self.ncols, self.nnz, self.rb, self.cb = nrows, ncols, nnz, rb, cb
+        self.nbr = (nrows + rb - 1) // rb
+
+    def fill(self, dtype: str, d_values: int, d_browptr: int, d_bcolind: int, d_bval: int, d_nnz_per_block: int,
+             stream: int = 0) -> None:
+        f = getattr(lib(), f"sparsep_csr2bcsr_device_{dtype}")
+        f.argtypes = [C.c_void_p] * 7
+        check(f(self.h, d_values, d_browptr, d_bcolind, d_bval, d_nnz_per_block, C.c_void_p(stream)),
+              f"csr2bcsr_device_{dtype}")
+
+    def free(self) -> None:
+        if self.h:
+            lib().sparsep_bcsr_layout_free(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

@@ -1390,6 +1390,58 @@ static int plan_csr_device(uint32_t nrows, uint32_t ncols, uint32_t nnz, const u
   return plan_csr<T>(&A, o, out, true);
 }
 
+// A plan from a BCSR matrix already on the device (the device converter's
+// output, or any BCSR of the reference layout): the block row pointers -- and,
+// for nnz-balanced parts, the nonzeros per block -- are read back for the
+// planner, the block columns checked on the device, the arrays copied into the
+// plan (the caller keeps its own).
+template <typename T>
+static int plan_bcsr_device(uint32_t nrows, uint32_t ncols, uint32_t rb, uint32_t cb, uint64_t nblocks, uint64_t nnz,
+                            const uint32_t *d_browptr, const uint32_t *d_bcolind, const T *d_bval,
+                            const uint32_t *d_nnz_per_block, const sparsep_opts *o, sparsep_plan **out) {
+  if (!out) return SPARSEP_EINVAL;
+  *out = nullptr;
+  if (!d_browptr || rb == 0 || cb == 0 || nblocks > UINT32_MAX || (nblocks && (!d_bcolind || !d_bval)))
+    return SPARSEP_EINVAL;
+  sparsep_opts oo;
+  if (o) oo = *o; else sparsep_opts_default(&oo);
+  if (int st = check_opts(&oo)) return st;
+  const uint32_t nbr = (uint32_t)(((uint64_t)nrows + rb - 1) / rb);
+  const uint32_t nbc = (uint32_t)(((uint64_t)ncols + cb - 1) / cb);
+  std::vector<uint32_t> bp((size_t)nbr + 1);
+  CK(cudaMemcpy(bp.data(), d_browptr, bp.size() * 4, cudaMemcpyDeviceToHost));
+  if (bp[0] != 0 || bp[nbr] != nblocks) return SPARSEP_EINVAL;
+  for (uint32_t i = 0; i < nbr; ++i)
+    if (bp[i] > bp[i + 1]) return SPARSEP_EINVAL;
+  if (nblocks) {
+    int *bad = nullptr, h = 0;
+    CK(cudaMalloc(&bad, sizeof(int)));
+    cudaError_t e = cudaMemset(bad, 0, sizeof(int));
+    if (e == cudaSuccess) {
+      cols_in_range<<<std::min<uint64_t>(4096, (nblocks + 255) / 256), 256>>>(d_bcolind, nblocks, nbc, bad);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h, bad, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    CK(e);
+    if (h) return SPARSEP_EINVAL;
+  }
+  std::vector<uint32_t> npb;
+  const bool need_npb = oo.nr_parts > 0 && oo.part_balance != SPARSEP_BAL_ROW && oo.part_balance != SPARSEP_BAL_BLOCK;
+  if (need_npb) {
+    if (!d_nnz_per_block) return SPARSEP_EINVAL;
+    npb.resize(nblocks);
+    if (nblocks) CK(cudaMemcpy(npb.data(), d_nnz_per_block, nblocks * 4, cudaMemcpyDeviceToHost));
+  }
+  Tile t;
+  t.row_end = nrows;
+  std::vector<uint32_t> sp;
+  if (oo.nr_parts > 0) sp = bcsr_split(oo, bp.data(), nbr, need_npb ? npb.data() : nullptr, oo.nr_parts);
+  else sp = {0, nbr};
+  return plan_bcsr_tiles<T>(SPARSEP_1D, nrows, ncols, nnz, nblocks, rb, cb, 1, bp.data(), (size_t)nbr + 1, d_bcolind,
+                            d_bval, {t}, {sp}, oo, out);
+}
+
 // ---------------------------------------------------------------------------
 // C-ABI
 // ---------------------------------------------------------------------------
@@ -1611,3 +1663,23 @@ SPARSEP_PLAN_DEVICE_ENTRY(int32_t, i32)
 SPARSEP_PLAN_DEVICE_ENTRY(int64_t, i64)
 SPARSEP_PLAN_DEVICE_ENTRY(float, f32)
 SPARSEP_PLAN_DEVICE_ENTRY(double, f64)
+
+#define SPARSEP_PLAN_BCSR_DEVICE_ENTRY(T, S)                                                                       \
+  extern "C" int sparsep_plan_bcsr_device_##S(uint32_t nrows, uint32_t ncols, uint32_t rb, uint32_t cb,           \
+                                              uint64_t nblocks, uint64_t nnz, const uint32_t *d_browptr,          \
+                                              const uint32_t *d_bcolind, const T *d_bval,                         \
+                                              const uint32_t *d_nnz_per_block, const sparsep_opts *o,             \
+                                              sparsep_plan **out) {                                               \
+    try {                                                                                                          \
+      return plan_bcsr_device<T>(nrows, ncols, rb, cb, nblocks, nnz, d_browptr, d_bcolind, d_bval, d_nnz_per_block, \
+                                 o, out);                                                                          \
+    } catch (const std::bad_alloc &) {                                                                             \
+      return SPARSEP_ENOMEM;                                                                                       \
+    }                                                                                                              \
+  }
+SPARSEP_PLAN_BCSR_DEVICE_ENTRY(int8_t, i8)
+SPARSEP_PLAN_BCSR_DEVICE_ENTRY(int16_t, i16)
+SPARSEP_PLAN_BCSR_DEVICE_ENTRY(int32_t, i32)
+SPARSEP_PLAN_BCSR_DEVICE_ENTRY(int64_t, i64)
+SPARSEP_PLAN_BCSR_DEVICE_ENTRY(float, f32)
+SPARSEP_PLAN_BCSR_DEVICE_ENTRY(double, f64)
