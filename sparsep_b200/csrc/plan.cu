@@ -1500,12 +1500,12 @@ int sparsep_device_sms(void) {
 void sparsep_plan_free(sparsep_plan *p) {
   if (!p) return;
   if (p->stream) cudaStreamSynchronize(p->stream);
-  for (void *d : p->allocs) cudaFree(d);
-  if (p->h_err) cudaFreeHost(p->h_err);
   if (p->copy_stream) {
     cudaStreamSynchronize(p->copy_stream);
     cudaStreamDestroy(p->copy_stream);
   }
+  for (void *d : p->allocs) cudaFree(d);
+  if (p->h_err) cudaFreeHost(p->h_err);
   if (p->band_ev) cudaEventDestroy(p->band_ev);
   for (auto &e : p->ev)
     if (e) cudaEventDestroy(e);
@@ -1570,9 +1570,15 @@ int sparsep_execute_host(sparsep_plan *p, const void *h_x, void *h_y) {
     if (int st = run_any(p, p->xpad, p->y, s, p->band_cnt)) return st;
     CK(cudaEventRecord(p->ev[2], s));
     CK(cudaEventRecord(p->ev[3], s));
-    if (int st = copy_y_banded(p, h_y)) return st;
+    const int cst = copy_y_banded(p, h_y);
+    // the copy stream is drained before the call returns, also when a copy
+    // failed: no band wait may outlive this call and read the next call's counters
     CK(cudaEventRecord(p->ev[4], p->copy_stream));
     CK(cudaStreamWaitEvent(s, p->ev[4], 0));
+    if (cst) {
+      cudaStreamSynchronize(s);
+      return cst;
+    }
   } else {
     if (int st = run_any(p, p->xpad, p->y, s)) return st;
     if (p->out_mode != OUT_PARTIAL) CK(cudaEventRecord(p->ev[2], s));
