@@ -44,6 +44,33 @@ int run_cg(const char *mtx, const void *d_b, void *d_x) {
   return st;
 }
 
+/* Device CSR -> 4x4 BCSR -> plan -> SpMV without the matrix leaving the GPU;
+ * dalloc is the caller's device allocator (the library's own buffers are
+ * inside the layout and the plan). */
+typedef void *(*dev_alloc_fn)(size_t bytes);
+int run_device_bcsr(const uint32_t *d_rowptr, const uint32_t *d_colind, const float *d_vals, uint32_t nrows,
+                    uint32_t ncols, uint32_t nnz, dev_alloc_fn dalloc, const float *d_x, float *d_y) {
+  sparsep_bcsr_layout *layout = NULL;
+  sparsep_plan *plan = NULL;
+  uint64_t nb = 0;
+  uint32_t *bp = NULL, *bc = NULL, *npb = NULL;
+  float *bv = NULL;
+  int st = sparsep_bcsr_layout_device(d_rowptr, d_colind, nrows, ncols, nnz, 4, 4, &layout, &nb, NULL);
+  if (!st) {
+    bp = dalloc(((size_t)(nrows + 3) / 4 + 1) * sizeof(uint32_t));
+    bc = dalloc((size_t)nb * sizeof(uint32_t) + 4);
+    bv = dalloc((size_t)nb * 16 * sizeof(float) + 4);
+    npb = dalloc((size_t)nb * sizeof(uint32_t) + 4);
+    if (!bp || !bc || !bv || !npb) st = SPARSEP_ENOMEM;
+  }
+  if (!st) st = sparsep_csr2bcsr_device_f32(layout, d_vals, bp, bc, bv, npb, NULL);
+  sparsep_bcsr_layout_free(layout);
+  if (!st) st = sparsep_plan_bcsr_device_f32(nrows, ncols, 4, 4, nb, nnz, bp, bc, bv, npb, NULL, &plan);
+  if (!st) st = sparsep_execute_device(plan, d_x, d_y, NULL);
+  sparsep_plan_free(plan);
+  return st;
+}
+
 int main(int argc, char **argv) {
   (void)argc;
   (void)argv;
