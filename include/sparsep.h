@@ -361,7 +361,7 @@ int sparsep_execute_device(sparsep_plan *plan, const void *d_x, void *d_y, void 
 
 /* Execute with HOST pointers: H2D x, kernel(s), D2H y, synchronous.  Fills the
  * timer slots 1..4.  1D CSR plans with at least 1 MB of y copy y back in up to
- * 8 row bands (info.y_bands), each as soon as the kernel has finished the
+ * 4 row bands (info.y_bands), each as soon as the kernel has finished the
  * items writing it; slot 3 is then the part of the copy left after the
  * kernel.  A pinned y buffer lets the band copies run without host waits. */
 int sparsep_execute_host(sparsep_plan *plan, const void *h_x, void *h_y);

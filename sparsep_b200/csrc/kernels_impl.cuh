@@ -729,12 +729,16 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
   }
 
   // Host-buffer path: the item is counted in its row band once all of its
-  // writes to y are visible device-wide; a copy stream waiting on the band's
-  // count moves those rows to the host while later items still run.
+  // writes to y are visible device-wide (barrier, then one fence before the
+  // count: the fence is cumulative over the writes the barrier ordered before
+  // it); a copy stream waiting on the band's count moves those rows to the
+  // host while later items still run.
   if (P.band_cnt != nullptr) {
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(P.band_cnt + it.band, 1u);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(P.band_cnt + it.band, 1u);
+    }
   }
 }
 

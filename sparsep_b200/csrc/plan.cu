@@ -30,8 +30,11 @@ using namespace sparsep;
 // ---------------------------------------------------------------------------
 // plan object
 // ---------------------------------------------------------------------------
-// Row bands of y for the host-buffer path (each >= BAND_MIN_BYTES of y).
-static constexpr uint32_t MAX_BANDS = 8;
+// Row bands of y for the host-buffer path (each >= BAND_MIN_BYTES of y).  Each
+// band's wait and copy cost ~8 us on a B200 (32 bands of 4 MB: 249 us exposed),
+// so few large bands win: 4 bands leave 37 us of a 4 MB copy after the kernel,
+// 8 bands 62 us, one copy 84 us.
+static constexpr uint32_t MAX_BANDS = 4;
 static constexpr size_t BAND_MIN_BYTES = 512 * 1024;
 
 struct sparsep_plan {
@@ -60,9 +63,9 @@ struct sparsep_plan {
   uint32_t nbands = 0;
   uint32_t band_row[MAX_BANDS + 1] = {};  // band b = rows [band_row[b], band_row[b+1])
   uint32_t band_items[MAX_BANDS] = {};    // items of band b: the count its copy waits for
-  unsigned int *band_cnt = nullptr;       // device counters, cleared before each launch
+  unsigned int *band_cnt = nullptr;       // device counters: items finished, over all host calls
+  uint32_t band_calls = 0;                // host calls whose kernel was launched (mod 2^32)
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t band_ev = nullptr;          // counters cleared (on the plan's stream)
   unsigned int *row_cnt = nullptr;  // long-row arrival counters (pipelined CSR)
   uint64_t n_rowptr = 0, n_idx = 0, n_val = 0, n_elems = 0;  // allocated extents
   bool stage = false;
@@ -388,7 +391,6 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
     st = dalloc(p, MAX_BANDS * sizeof(unsigned int), (void **)&p->band_cnt);
     if (st) return st;
     CK(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&p->band_ev, cudaEventDisableTiming));
   }
   uint32_t nlong = 0;
   for (const Item &it : items) nlong += it.kind == ITEM_LONG && it.chunk == 0;
@@ -1506,7 +1508,6 @@ void sparsep_plan_free(sparsep_plan *p) {
   }
   for (void *d : p->allocs) cudaFree(d);
   if (p->h_err) cudaFreeHost(p->h_err);
-  if (p->band_ev) cudaEventDestroy(p->band_ev);
   for (auto &e : p->ev)
     if (e) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -1535,7 +1536,10 @@ int sparsep_execute_device(sparsep_plan *p, const void *d_x, void *d_y, void *st
 
 // y in row bands: each band's copy, on the plan's copy stream, waits
 // (cuStreamWaitValue32) until the kernel has counted all items of the band, so
-// the copies of the early bands overlap the kernel's later items.
+// the copies of the early bands overlap the kernel's later items.  The
+// counters are never cleared: after the n-th launch counter b holds
+// n * band_items[b] (mod 2^32, which the wait's wrap-around comparison
+// handles), so a wait for call n cannot be met by an earlier call's counts.
 static int copy_y_banded(sparsep_plan *p, void *h_y) {
   cudaStream_t c = p->copy_stream;
   const size_t es = p->esize;
@@ -1543,8 +1547,8 @@ static int copy_y_banded(sparsep_plan *p, void *h_y) {
   const char *dy = static_cast<const char *>(p->y);
   uint32_t b = 0;
   for (; b < p->nbands; ++b) {
-    if (wait_value32()(c, (CUdeviceptr)(uintptr_t)(p->band_cnt + b), p->band_items[b], CU_STREAM_WAIT_VALUE_GEQ) !=
-        CUDA_SUCCESS)
+    const cuuint32_t target = p->band_calls * p->band_items[b];
+    if (wait_value32()(c, (CUdeviceptr)(uintptr_t)(p->band_cnt + b), target, CU_STREAM_WAIT_VALUE_GEQ) != CUDA_SUCCESS)
       break;
     const size_t r0 = p->band_row[b], r1 = p->band_row[b + 1];
     if (r1 > r0) CK(cudaMemcpyAsync(hy + r0 * es, dy + r0 * es, (r1 - r0) * es, cudaMemcpyDeviceToHost, c));
@@ -1564,10 +1568,8 @@ int sparsep_execute_host(sparsep_plan *p, const void *h_x, void *h_y) {
   CK(cudaMemcpyAsync(p->xpad, h_x, (size_t)p->ncols * p->esize, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(p->ev[1], s));
   if (p->nbands) {
-    CK(cudaMemsetAsync(p->band_cnt, 0, p->nbands * sizeof(unsigned int), s));
-    CK(cudaEventRecord(p->band_ev, s));
-    CK(cudaStreamWaitEvent(p->copy_stream, p->band_ev, 0));  // counters cleared before any wait reads them
     if (int st = run_any(p, p->xpad, p->y, s, p->band_cnt)) return st;
+    ++p->band_calls;  // the launch adds band_items[b] to counter b
     CK(cudaEventRecord(p->ev[2], s));
     CK(cudaEventRecord(p->ev[3], s));
     const int cst = copy_y_banded(p, h_y);
