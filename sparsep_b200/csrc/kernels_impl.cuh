@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
-      atomicAdd(P.band_cnt + it.band, 1u);
+      atomicAdd(P.band_cnt + P.items[item_id].band, 1u);  // re-read: keeps the band out of the body's registers
     }
   }
 }
