@@ -656,6 +656,20 @@ int sparsep_cg_solve(sparsep_cg *cg, const void *d_b, void *d_x, uint32_t max_it
                      uint32_t check_every, uint32_t *iters, double *rel_residual, void *stream);
 void sparsep_cg_free(sparsep_cg *cg);
 
+/* Power iteration on a square FP32 / FP64 plan (ENOSYS for integer plans):
+ * d_x (n device elements) holds the start vector and receives the unit-norm
+ * estimate of the dominant eigenvector.  Each iteration -- SpMV, the Rayleigh
+ * quotient lambda = p . Ap and ||Ap|| as fixed-order double sums, p = Ap/||Ap||
+ * -- is one CUDA graph replayed on `stream`; lambda is read back every
+ * check_every iterations and the run stops when two reads differ by at most
+ * rel_tol * |lambda| (or A p = 0, or after max_iters).  Bit-identical from run
+ * to run. */
+typedef struct sparsep_power sparsep_power;
+int sparsep_power_create(sparsep_plan *plan, sparsep_power **out);
+int sparsep_power_run(sparsep_power *pw, void *d_x, uint32_t max_iters, double rel_tol, uint32_t check_every,
+                      double *lambda, uint32_t *iters, void *stream);
+void sparsep_power_free(sparsep_power *pw);
+
 /* ------------------------------------------------------------------------ */
 /* Learned variant selector (no reference counterpart)                       */
 /* ------------------------------------------------------------------------ */

@@ -748,3 +748,38 @@ class CG:
             self.free()
         except Exception:
             pass
+
+
+class PowerIteration:
+    """Power iteration (sparsep_power_*) on a square FP32 / FP64 plan."""
+
+    def __init__(self, plan: "Plan"):
+        L = lib()
+        L.sparsep_power_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        L.sparsep_power_run.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32,
+                                        C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.c_void_p]
+        L.sparsep_power_free.argtypes = [C.c_void_p]
+        L.sparsep_power_free.restype = None
+        self.plan = plan
+        h = C.c_void_p()
+        check(L.sparsep_power_create(plan.h, C.byref(h)), "power_create")
+        self.h = h
+
+    def run(self, d_x: int, max_iters: int = 1000, rel_tol: float = 1e-10, check_every: int = 10,
+            stream: int | None = None):
+        """Iterate in place on the device vector d_x; returns (lambda, iterations)."""
+        lam, it = C.c_double(), C.c_uint32()
+        check(lib().sparsep_power_run(self.h, C.c_void_p(d_x), max_iters, rel_tol, check_every, C.byref(lam),
+                                      C.byref(it), C.c_void_p(stream) if stream else None), "power_run")
+        return lam.value, it.value
+
+    def free(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().sparsep_power_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

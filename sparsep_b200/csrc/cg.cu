@@ -1,5 +1,6 @@
-// cg.cu -- conjugate gradient on a plan: the iterative-solver caller of the
-// SpMV (no counterpart in the reference, whose programs run one SpMV).
+// cg.cu -- conjugate gradient and power iteration on a plan: the iterative
+// callers of the SpMV (no counterpart in the reference, whose programs run one
+// SpMV).
 //
 // One CG iteration is the plan's SpMV q = A p followed by four small kernels:
 //   dot   p . q                      (per-CTA partial sums)
@@ -24,7 +25,7 @@ namespace cg {
 
 constexpr int NT = 256;   // threads per CTA of the vector kernels
 constexpr int NB = 592;   // CTAs of the vector kernels (4 per SM of a B200)
-enum { S_RR = 0, S_PQ = 1, S_BETA = 2, S_BB = 3, S_NSC = 4 };
+enum { S_RR = 0, S_PQ = 1, S_BETA = 2, S_BB = 3, S_QQ = 4, S_NSC = 5 };
 
 __device__ __forceinline__ double block_sum(double v, double *sm) {
   sm[threadIdx.x] = v;
@@ -110,6 +111,16 @@ __global__ void __launch_bounds__(NT) update_p(T *__restrict__ p, const T *__res
                                                const double *__restrict__ sc) {
   const T beta = (T)sc[S_BETA];
   for (size_t i = (size_t)blockIdx.x * NT + threadIdx.x; i < n; i += (size_t)NB * NT) p[i] = r[i] + beta * p[i];
+}
+
+// power iteration: p = q / ||q|| with ||q||^2 in sc[slot] (p unchanged when q = 0);
+// p and q may be the same vector
+template <typename T>
+__global__ void __launch_bounds__(NT) normalise(T *p, const T *q, size_t n, const double *__restrict__ sc, int slot) {
+  const double qq = sc[slot];
+  if (!(qq > 0.0)) return;
+  const T inv = (T)(1.0 / std::sqrt(qq));
+  for (size_t i = (size_t)blockIdx.x * NT + threadIdx.x; i < n; i += (size_t)NB * NT) p[i] = q[i] * inv;
 }
 
 }  // namespace cg
@@ -203,6 +214,83 @@ static int solve(sparsep_cg *c, const T *b, T *x, uint32_t max_iters, double tol
   return SPARSEP_OK;
 }
 
+// Power iteration: p_0 = x / ||x||; per iteration q = A p, lambda = p . q
+// (the Rayleigh quotient, p having unit norm), p = q / ||q||.  The iteration is
+// one captured graph (SpMV, two fixed-order dot products, the normalisation);
+// the host reads lambda every check_every iterations and stops when two reads
+// differ by at most rel_tol * |lambda|.  x receives the last p.
+struct sparsep_power {
+  sparsep_plan *plan = nullptr;
+  int dtype = 0;
+  size_t n = 0;
+  void *q = nullptr;
+  double *part = nullptr, *sc = nullptr;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void *graph_x = nullptr;
+};
+
+template <typename T>
+static int power_step(sparsep_power *w, T *p, cudaStream_t s) {
+  if (int st = sparsep_execute_device(w->plan, p, w->q, s)) return st;
+  const T *q = static_cast<const T *>(w->q);
+  dot<T><<<NB, NT, 0, s>>>(p, q, w->n, w->part);
+  finish<<<1, NT, 0, s>>>(w->part, w->sc, S_PQ);
+  dot<T><<<NB, NT, 0, s>>>(q, q, w->n, w->part);
+  finish<<<1, NT, 0, s>>>(w->part, w->sc, S_QQ);
+  normalise<T><<<NB, NT, 0, s>>>(p, q, w->n, w->sc, S_QQ);
+  return cg_err(cudaGetLastError());
+}
+
+template <typename T>
+static int power_run(sparsep_power *w, T *x, uint32_t max_iters, double tol, uint32_t check_every, double *lambda,
+                     uint32_t *iters, cudaStream_t s) {
+  // p_0 = x / ||x||, in place
+  dot<T><<<NB, NT, 0, s>>>(x, x, w->n, w->part);
+  finish<<<1, NT, 0, s>>>(w->part, w->sc, S_QQ);
+  normalise<T><<<NB, NT, 0, s>>>(x, x, w->n, w->sc, S_QQ);
+  CGK(cudaGetLastError());
+  if (!w->exec || w->graph_x != (void *)x) {
+    if (w->exec) cudaGraphExecDestroy(w->exec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    w->exec = nullptr;
+    w->graph = nullptr;
+    CGK(cudaStreamBeginCapture(w->cap, cudaStreamCaptureModeThreadLocal));
+    const int st = power_step<T>(w, x, w->cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(w->cap, &g);
+    if (st) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    CGK(e);
+    w->graph = g;
+    CGK(cudaGraphInstantiate(&w->exec, w->graph, 0));
+    w->graph_x = x;
+  }
+  double h[S_NSC];
+  uint32_t it = 0;
+  double prev = 0.0, lam = 0.0;
+  bool have_prev = false;
+  const uint32_t every = check_every ? check_every : 1;
+  while (it < max_iters) {
+    const uint32_t k = std::min(every, max_iters - it);
+    for (uint32_t j = 0; j < k; ++j) CGK(cudaGraphLaunch(w->exec, s));
+    it += k;
+    CGK(cudaMemcpyAsync(h, w->sc, sizeof h, cudaMemcpyDeviceToHost, s));
+    CGK(cudaStreamSynchronize(s));
+    lam = h[S_PQ];
+    if (!(h[S_QQ] > 0.0)) break;  // A p = 0: lambda = 0 and nothing left to iterate
+    if (have_prev && std::fabs(lam - prev) <= tol * std::fabs(lam)) break;
+    prev = lam;
+    have_prev = true;
+  }
+  if (lambda) *lambda = lam;
+  if (iters) *iters = it;
+  return SPARSEP_OK;
+}
+
 extern "C" {
 
 int sparsep_cg_create(sparsep_plan *plan, sparsep_cg **out) {
@@ -251,6 +339,51 @@ int sparsep_cg_solve(sparsep_cg *c, const void *d_b, void *d_x, uint32_t max_ite
     return solve<float>(c, (const float *)d_b, (float *)d_x, max_iters, rel_tol, check_every, iters, rel_residual, s);
   return solve<double>(c, (const double *)d_b, (double *)d_x, max_iters, rel_tol, check_every, iters, rel_residual,
                        s);
+}
+
+int sparsep_power_create(sparsep_plan *plan, sparsep_power **out) {
+  if (!plan || !out) return SPARSEP_EINVAL;
+  *out = nullptr;
+  sparsep_plan_info info;
+  if (int st = sparsep_plan_get_info(plan, &info)) return st;
+  if (info.nrows != info.ncols) return SPARSEP_EINVAL;
+  if (info.dtype != SPARSEP_FP32 && info.dtype != SPARSEP_FP64) return SPARSEP_ENOSYS;
+  auto *w = new (std::nothrow) sparsep_power();
+  if (!w) return SPARSEP_ENOMEM;
+  w->plan = plan;
+  w->dtype = info.dtype;
+  w->n = info.nrows;
+  const size_t es = info.dtype == SPARSEP_FP32 ? 4 : 8;
+  int st = cg_err(cudaMalloc(&w->q, (w->n + 64) * es));
+  if (!st) st = cg_err(cudaMalloc(&w->part, sizeof(double) * NB));
+  if (!st) st = cg_err(cudaMalloc(&w->sc, sizeof(double) * S_NSC));
+  if (!st) st = cg_err(cudaMemset(w->sc, 0, sizeof(double) * S_NSC));
+  if (!st) st = cg_err(cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking));
+  if (st) {
+    sparsep_power_free(w);
+    return st;
+  }
+  *out = w;
+  return SPARSEP_OK;
+}
+
+void sparsep_power_free(sparsep_power *w) {
+  if (!w) return;
+  if (w->exec) cudaGraphExecDestroy(w->exec);
+  if (w->graph) cudaGraphDestroy(w->graph);
+  for (void *d : {w->q, (void *)w->part, (void *)w->sc})
+    if (d) cudaFree(d);
+  if (w->cap) cudaStreamDestroy(w->cap);
+  delete w;
+}
+
+int sparsep_power_run(sparsep_power *w, void *d_x, uint32_t max_iters, double rel_tol, uint32_t check_every,
+                      double *lambda, uint32_t *iters, void *stream) {
+  if (!w || !d_x || !(rel_tol >= 0.0)) return SPARSEP_EINVAL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (w->dtype == SPARSEP_FP32)
+    return power_run<float>(w, (float *)d_x, max_iters, rel_tol, check_every, lambda, iters, s);
+  return power_run<double>(w, (double *)d_x, max_iters, rel_tol, check_every, lambda, iters, s);
 }
 
 }  // extern "C"
