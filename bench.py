@@ -367,6 +367,128 @@ def run_batch(args):
             "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
 
 
+# ---------------------------------------------------------------------------
+# Every benchmark configuration: one device-timed number and one check each
+# ---------------------------------------------------------------------------
+# The reference directory whose spmv_host multiplies each struct kind
+REF_DIR = {"csr": "1D_CSR_row", "cooe": "1D_COO_nnz", "bcsr": "1D_BCSR_nnz", "bcoo": "1D_BCOO_nnz",
+           "dcsr": "2D_DCSR", "rbdcsr": "2D_RBDCSR", "bdcsr": "2D_BDCSR", "dcoo": "2D_DCOO", "rbdcoo": "2D_RBDCOO",
+           "bdcoo": "2D_BDCOO"}
+
+
+class RefHost:
+    """The reference's own host SpMV for a struct kind and element type
+    (spmv_host of that kind's host/app.c, built from the reference sources
+    into oracle/_ref), else the oracle's restatement of it.  Used for the
+    CPU baseline of each configuration and, with its result, as the check."""
+
+    def __init__(self, kind, dtype):
+        so = ROOT / "oracle" / "_ref" / f"libref_{REF_DIR[kind]}_{dtype}.so"
+        if so.exists():
+            self.fn, self.kind = C.CDLL(str(so)).ref_spmv, "reference"
+        else:
+            port = ROOT / "oracle" / "liboracle.so"
+            if not port.exists():
+                subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "liboracle.so"], check=True)
+            self.fn, self.kind = getattr(C.CDLL(str(port)), f"oracle_spmv_{kind}_{dtype}"), "port"
+
+    @staticmethod
+    def lengths(A):
+        """(x length, y length) the reference's host code reads and writes."""
+        s = A.s
+        if A.kind in ("bcsr", "bcoo"):
+            return int(s.ncols) + 16, int(s.num_block_rows * s.row_block_size)
+        if A.kind in ("dcsr", "dcoo"):
+            return int(s.vert_partitions * s.tile_width) + 8, int(s.horz_partitions * s.tile_height)
+        return int(s.ncols) + 16, int(s.nrows)
+
+    def run(self, A, x, passes=1):
+        """y and the seconds per pass of the reference's SpMV on A and x."""
+        xl, yl = self.lengths(A)
+        xp = np.zeros(max(xl, x.size), dtype=x.dtype)
+        xp[: x.size] = x
+        y = np.zeros(yl + 8, dtype=x.dtype)
+        t0 = time.perf_counter()
+        for _ in range(passes):
+            self.fn(y.ctypes.data_as(C.c_void_p), A.ref, xp.ctypes.data_as(C.c_void_p))
+        return y[: int(A.s.nrows)].copy(), (time.perf_counter() - t0) / passes
+
+
+def fp_check(y, y_ref, y_abs, counts, dtype):
+    """|y - y_ref| <= 2 gamma_n sum|a x| per row: both are sums of the same
+    products, each within gamma_n sum|a x| of the exact value.  y_abs is the
+    reference's own sum of |a||x| in the element type (within gamma_n of exact,
+    covered by the 1.01 factor).  Returns (ok, max err / bound)."""
+    u = 2.0 ** -24 if dtype == "f32" else 2.0 ** -53
+    n = np.maximum(counts.astype(np.float64), 1.0)
+    bound = 1.01 * 2 * (n * u / (1 - n * u)) * y_abs.astype(np.float64) + 1e-300
+    err = np.abs(y.astype(np.float64) - y_ref.astype(np.float64))
+    r = err / bound
+    return bool((r <= 1.0).all()), float(r.max()) if r.size else 0.0
+
+
+def time_device(plan, xd, yd, stream, flush, reps):
+    """Median device time (ms) of plan on x/y with L2 flushed before each run."""
+    import torch
+
+    for _ in range(3):
+        flush.zero_()
+        plan.run_device(xd.data_ptr(), yd.data_ptr(), stream.cuda_stream)
+    ts = []
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.run_device(xd.data_ptr(), yd.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def measure_struct(cfg, workload, A, A_abs, x, counts, cases, peak, stream, flush, reps=10, ref_budget_s=2.0):
+    """One struct: the reference's host SpMV once (CPU baseline, and its y as
+    the check), then every option set in `cases` planned, device-timed and
+    checked: integers bit for bit against the reference, FP within
+    2 gamma_n sum|a x| of it.  A_abs: the same struct with |values| (FP)."""
+    import torch
+
+    import sparsep_b200 as sp
+
+    dt = A.dtype
+    ref = RefHost(A.kind, dt)
+    y_ref, sec = ref.run(A, x)
+    passes = max(1, min(10, int(ref_budget_s / max(sec, 1e-6))))
+    if passes > 1:
+        sec = ref.run(A, x, passes)[1]
+    y_abs = ref.run(A_abs, np.abs(x))[0] if dt in ("f32", "f64") else None
+    xd = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    yd = torch.empty(int(A.s.nrows), dtype=xd.dtype, device="cuda")
+    out = []
+    for name, o in cases:
+        plan = sp.Plan(A, sp.default_opts(**o))
+        ms = time_device(plan, xd, yd, stream, flush, reps)
+        y = yd.cpu().numpy()
+        cb = int(plan.info.compulsory_bytes)
+        if y_abs is None:
+            ok, check = bool(np.array_equal(y, y_ref)), "bit-exact vs reference spmv_host"
+        else:
+            ok, r = fp_check(y, y_ref, y_abs, counts, dt)
+            check = f"max |y - y_ref| / (2 gamma_n sum|ax|) = {r:.3g}"
+        gbs = cb / (ms * 1e-3) / 1e9
+        out.append({"config": cfg, "workload": workload, "dtype": dt, "kind": A.kind, "case": name,
+                    "variant": plan.info.variant.decode(), "us": round(ms * 1e3, 2), "gbs": round(gbs, 1),
+                    "frac": round(gbs / peak, 4), "compulsory_bytes": cb, "check_ok": ok, "check": check,
+                    "cpu_baseline": {"value": round(cb / sec / 1e9, 3), "unit": "GB/s", "cores": 1,
+                                     "kind": ref.kind, "ms_per_spmv": round(sec * 1e3, 2),
+                                     "sample": f"{passes} full pass(es) of spmv_host ({REF_DIR[A.kind]})"}})
+        log(f"[bench] C{cfg} {workload} {dt} {A.kind} {name}: {ms * 1e3:.1f} us, {gbs:.0f} GB/s, "
+            f"ok={ok} ({check})")
+        plan.free()
+    del xd, yd
+    return out
+
+
 def _ref_csr_lib():
     so = ROOT / "oracle" / "_ref" / "libref_1D_CSR_row_f32.so"
     if so.exists():

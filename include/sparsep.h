@@ -115,7 +115,13 @@ typedef struct sparsep_opts {
   int32_t stage_x;         /* 2D: stage the x-segment in shared memory (1/0/-1=auto) */
   int32_t item_nnz;        /* auto plans: target nonzeros per CTA work item (0 = auto) */
   int32_t pipeline;        /* 1D CSR auto plans: 1 = persistent TMA-pipelined kernel */
-  int32_t reserved[1];
+  int32_t autotune;        /* 0 = the options as given; 1 = learned choice of the
+                              plan variant with exhaustive fallback; 2 = exhaustive */
+  int32_t heavy_rows;      /* 1D CSR auto plans: rows with at least this many
+                              nonzeros run in column stripes whose x segment is
+                              staged in shared memory (0 = planner's choice,
+                              -1 = never) */
+  int32_t reserved[2];
 } sparsep_opts;
 
 /* Defaults: 1D, nnz balance, auto parts/workers/lanes, LF, nrhs = 1. */
@@ -730,8 +736,12 @@ int sparsep_batch_select(sparsep_batch *b, sparsep_selector *s, float min_confid
  * most 2^28 nonzeros (larger inputs return SPARSEP_ERANGE), that every GPU
  * loading the library holds until exit.  The first call on a device looks
  * the array up (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race,
- * so serialise them (one stream, or events). */
+ * capture; after a device reset the next call looks it up again.  All calls
+ * share the array: calls that overlap on the GPU race, so serialise them
+ * (one stream, or events).  Unchecked preconditions (the call does no pass
+ * over the input): entries sorted by row, rowind < nrows and colind < ncols.
+ * A row index out of range writes nothing; a column index out of range reads
+ * outside d_x (undefined). */
 int sparsep_spmv_cooe_f32_noalloc(const sparsep_elem_f32 *d_elems, uint32_t nnz, uint32_t nrows, uint32_t ncols,
                                   const float *d_x, float *d_y, void *stream);
 

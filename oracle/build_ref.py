@@ -15,6 +15,10 @@ plus -fwrapv, which pins the signed wrap-around of `sum += x * val` for
 int32/int64 that the reference relies on.
 
 Usage: python oracle/build_ref.py [reference_root]
+
+The reference root is the argument, else $SPARSEP_REFERENCE, else a
+directory named `reference` beside the repository; without a reference tree
+nothing is built.
 """
 from __future__ import annotations
 
@@ -238,8 +242,16 @@ def build_one(ref: Path, d: str, tag: str, macro: str) -> Path:
     return so
 
 
-def build(ref_root: str | os.PathLike = "/root/reference") -> list[Path]:
-    ref = Path(ref_root)
+def reference_root(arg: str | os.PathLike | None = None) -> Path:
+    """The reference tree: the argument, $SPARSEP_REFERENCE, or ../reference."""
+    if arg:
+        return Path(arg)
+    env = os.environ.get("SPARSEP_REFERENCE")
+    return Path(env) if env else HERE.parent.parent / "reference"
+
+
+def build(ref_root: str | os.PathLike | None = None) -> list[Path]:
+    ref = reference_root(ref_root)
     if not (ref / "spmv").is_dir():
         return []
     OUT.mkdir(parents=True, exist_ok=True)
@@ -249,5 +261,5 @@ def build(ref_root: str | os.PathLike = "/root/reference") -> list[Path]:
 
 
 if __name__ == "__main__":
-    libs = build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    libs = build(sys.argv[1] if len(sys.argv) > 1 else None)
     print(f"built {len(libs)} reference libraries into {OUT}")

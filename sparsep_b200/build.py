@@ -1,7 +1,7 @@
 """Build libsparsep_b200.so in-tree with nvcc for sm_100a.
 
-Sources: csrc/kernels.cu and csrc/csr_pipe.cu (compiled once per element
-type, in parallel), csrc/batch_kernels.cu (once per batched type), the other
+Sources: csrc/kernels.cu, csrc/csr_pipe.cu and csrc/csr_stripes.cu (compiled
+once per element type, in parallel), csrc/batch_kernels.cu (once per batched type), the other
 csrc/*.cu and csrc/*.cpp.  Objects go to sparsep_b200/_build/.
 """
 from __future__ import annotations
@@ -64,9 +64,9 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
     flags = NVCC_FLAGS + (["-DSPARSEP_CHECK"] if checked else [])
     jobs = []
     objs = []
-    per_type = ("kernels.cu", "csr_pipe.cu", "batch_kernels.cu")
+    per_type = ("kernels.cu", "csr_pipe.cu", "csr_stripes.cu", "batch_kernels.cu")
     for tag, ctype in KERNEL_TYPES.items():
-        for name in per_type[:2]:
+        for name in per_type[:3]:
             o = bdir / f"{Path(name).stem}_{tag}.o"
             objs.append(o)
             jobs.append([nvcc(), *ARCH, *flags, f"-DSPARSEP_KT={ctype}", "-c", str(CSRC / name), "-o", str(o)])

@@ -56,8 +56,8 @@ class Bind(C.Structure):
 class Opts(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "format", "scheme", "part_balance", "worker_balance", "sync", "nr_parts", "nr_workers",
-        "vert_partitions", "row_block_size", "col_block_size", "lanes", "nrhs", "stage_x", "item_nnz", "pipeline")] + [
-        ("reserved", C.c_int32 * 1)]
+        "vert_partitions", "row_block_size", "col_block_size", "lanes", "nrhs", "stage_x", "item_nnz", "pipeline",
+        "autotune", "heavy_rows")] + [("reserved", C.c_int32 * 2)]
 
 
 class PlanInfo(C.Structure):

@@ -15,8 +15,10 @@
 // the process exits.  Calls share it, so calls that overlap on the GPU race.
 // Each call derives its work items from blockIdx (4096 nonzeros each), so no
 // plan or item table is needed either.
-#include <atomic>
 #include <cstring>
+#include <mutex>
+
+#include <cuda.h>
 
 #include "kernels_impl.cuh"
 
@@ -39,9 +41,13 @@ __global__ void __launch_bounds__(256) coo_f32(Params<float> P, uint64_t nnz) {
   it.a1 = it.a0 + ELEMS_PER_ITEM < nnz ? it.a0 + ELEMS_PER_ITEM : nnz;
   it.ptr_base = it.nnz_base = 0;
   it.row_off = it.col_off = 0;
-  // item k owns the rows from its first nonzero's row to the next item's first row
-  it.own0 = k == 0 ? 0u : el[it.a0].rowind;
-  it.own1 = k + 1 == P.nitems ? P.nrows : el[it.a1].rowind;
+  // item k owns the rows from its first nonzero's row to the next item's first
+  // row (clamped to nrows: a row index out of range, which is the caller's
+  // error, then writes nothing instead of walking past y)
+  const uint32_t f0 = k == 0 ? 0u : el[it.a0].rowind, f1 = k + 1 == P.nitems ? P.nrows : el[it.a1].rowind;
+  it.own0 = f0 < P.nrows ? f0 : P.nrows;
+  it.own1 = f1 < P.nrows ? f1 : P.nrows;
+  if (it.own1 < it.own0) it.own1 = it.own0;
   it.xlo = it.xw = 0;
   it.slot = 0;
   it.kind = ITEM_ELEMS;
@@ -62,8 +68,28 @@ __global__ void __launch_bounds__(256) coo_f32(Params<float> P, uint64_t nnz) {
   }
 }
 
-// device address of g_scratch, looked up once per device
-static std::atomic<unsigned long long *> g_addr[64];
+// Device address of g_scratch, looked up once per device and context: a
+// device reset gives the device a new primary context (and the library's
+// device image a new address), so the lookup is redone when the current
+// context is not the one the address was found in.
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+static CtxGetCurrent ctx_get_current() {
+  static const CtxGetCurrent fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  return fn;
+}
+struct Slot {
+  CUcontext ctx = nullptr;
+  unsigned long long *addr = nullptr;
+};
+static Slot g_slot[64];
+static std::mutex g_mu;
 
 }  // namespace noalloc
 }  // namespace sparsep
@@ -88,13 +114,23 @@ extern "C" int sparsep_spmv_cooe_f32_noalloc(const sparsep_elem_f32 *d_elems, ui
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return noalloc_status(e);
   if (dev < 0 || dev >= 64) return SPARSEP_ENODEV;
-  unsigned long long *scratch = noalloc::g_addr[dev].load();
-  if (!scratch) {  // first call on this device (must come before any stream capture)
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, noalloc::g_scratch);
-    if (e != cudaSuccess) return noalloc_status(e);
-    scratch = static_cast<unsigned long long *>(p);
-    noalloc::g_addr[dev].store(scratch);
+  // set-up, once per device (and again after a device reset): the array's
+  // device address; the first call on a device should come before any
+  // stream capture
+  CUcontext ctx = nullptr;
+  if (noalloc::ctx_get_current() && noalloc::ctx_get_current()(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+  unsigned long long *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(noalloc::g_mu);
+    noalloc::Slot &sl = noalloc::g_slot[dev];
+    if (!sl.addr || sl.ctx != ctx) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, noalloc::g_scratch);
+      if (e != cudaSuccess) return noalloc_status(e);
+      sl.addr = static_cast<unsigned long long *>(p);
+      sl.ctx = ctx;
+    }
+    scratch = sl.addr;
   }
   if (nnz == 0) return noalloc_status(cudaMemsetAsync(d_y, 0, (size_t)nrows * sizeof(float), st));
   // the completion counter must start at zero

@@ -76,6 +76,21 @@ struct sparsep_plan {
   cudaEvent_t ev[5] = {};
   double t[5] = {0, 0, 0, 0, 0};
   sparsep_plan_info info{};
+  // Split 1D CSR plan: rows with >= `threshold` nonzeros (the heavy rows) run
+  // stripe-major in column stripes of W columns (csr_stripes.cu); the row
+  // kernels see the other rows only (rowptr, colind, val above hold them, with
+  // bit 31 of a heavy row's rowptr entry set).
+  struct Split {
+    bool on = false;
+    uint32_t threshold = 0, nH = 0, nS = 0, W = 0, ctas = 0, nchunks = 0;
+    uint64_t nnz = 0;  // heavy nonzeros
+    const uint32_t *hrow = nullptr, *vptr = nullptr, *cta_first = nullptr;
+    const uint16_t *hcol = nullptr;
+    const void *hval = nullptr;
+    const StripeChunk *chunks = nullptr;
+    void *part = nullptr;
+    uint64_t n_vptr = 0, n_h = 0, n_part = 0;
+  } split;
 };
 
 static thread_local char g_last_error[256] = "";
@@ -160,6 +175,7 @@ static int check_opts(const sparsep_opts *o) {
   if (o->part_balance < 0 || o->part_balance > SPARSEP_BAL_NNZ_ELEM) return SPARSEP_EINVAL;
   if (o->worker_balance < 0 || o->worker_balance > SPARSEP_BAL_INTERLEAVE) return SPARSEP_EINVAL;
   if (o->sync < 0 || o->sync > SPARSEP_SYNC_CG) return SPARSEP_EINVAL;
+  if (o->autotune < 0 || o->autotune > 2 || o->heavy_rows < -1) return SPARSEP_EINVAL;
   if (o->nrhs > 1) return SPARSEP_ENOSYS;
   return SPARSEP_OK;
 }
@@ -421,7 +437,7 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   p->info.nblocks = p->nblocks;
   p->info.items = p->nitems;
   p->info.device_bytes += p->info.scratch_bytes;
-  p->info.kernel_launches = 1 + (p->out_mode == OUT_PARTIAL ? 1 : 0);
+  p->info.kernel_launches = 1 + (p->out_mode == OUT_PARTIAL ? 1 : 0) + (p->split.on ? 2 : 0);
   p->info.workers = workers;
   p->info.stage_x = p->stage ? 1 : 0;
   p->info.y_bands = (int32_t)p->nbands;
@@ -435,9 +451,12 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   static const char *fm[] = {"csr", "coo", "bcsr", "bcoo"};
   static const char *sc[] = {"1d", "2d-d", "2d-rbd", "2d-bd"};
   static const char *sy[] = {"lf", "atomic", "atomic(cg)"};
-  std::snprintf(p->info.variant, sizeof p->info.variant, "%s/%s/%s/parts=%d/lanes=%s/V=%u%s%s", fm[p->format],
+  const std::string split =
+      p->split.on ? "/heavy>=" + std::to_string(p->split.threshold) + "x" + std::to_string(p->split.nS) + "stripes"
+                  : std::string();
+  std::snprintf(p->info.variant, sizeof p->info.variant, "%s/%s/%s/parts=%d/lanes=%s/V=%u%s%s%s", fm[p->format],
                 sc[p->scheme], sy[o.sync], o.nr_parts, o.lanes ? std::to_string(o.lanes).c_str() : "auto", p->V,
-                p->stage ? "/smem-x" : "", p->pipe ? "/tma-pipe" : "");
+                p->stage ? "/smem-x" : "", p->pipe ? "/tma-pipe" : "", split.c_str());
   // the uploads and clears above ran on the plan's stream: done before any
   // launch, on any stream, can read them
   CK(cudaStreamSynchronize(p->stream));
@@ -495,6 +514,192 @@ static void set_out_mode(sparsep_plan *p, const sparsep_opts &o, uint32_t V, boo
 }
 
 // ---------------------------------------------------------------------------
+// Split CSR plans: heavy rows in column stripes (csr_stripes.cu)
+// ---------------------------------------------------------------------------
+// Cost model of the planner's choice, in bytes of HBM streaming: a random x
+// gather through L2 costs about GATHER_BYTES (on a B200, 16.7 M gathers of a
+// 4 MB x take as long as streaming ~25 bytes each); a heavy nonzero costs its
+// 2-byte stripe column and value (its x is read from shared memory); each
+// stripe row costs its offset, its partial's store and the merge's read.
+static constexpr uint64_t GATHER_BYTES = 24;
+static constexpr uint64_t SPLIT_MIN_X_BYTES = 1 << 20;  // smaller x: gathers mostly hit L1
+// The planner chooses a split on its own only once the split path is measured
+// faster than the row kernel alone; until then heavy_rows > 0 requests it.
+static constexpr bool SPLIT_AUTO = false;
+
+static bool split_eligible(const sparsep_opts &o, uint64_t nnz) {
+  return o.heavy_rows >= 0 && o.lanes == 0 && o.pipeline != 1 && o.sync == SPARSEP_SYNC_LF && o.nrhs <= 1 &&
+         nnz < (1ull << 31);
+}
+
+// Heavy-row threshold for a split plan, 0 for none.
+static uint32_t split_threshold(const sparsep_opts &o, const uint32_t *rp, uint32_t nrows, uint32_t ncols, size_t s,
+                                uint32_t W) {
+  if (o.heavy_rows > 0) return (uint32_t)o.heavy_rows;
+  if (!SPLIT_AUTO || (uint64_t)ncols * s < SPLIT_MIN_X_BYTES || nrows == 0) return 0;
+  const uint64_t nS = (ncols + (uint64_t)W - 1) / W, nnz = rp[nrows];
+  // candidates: about 1, 2, 4, 8 nonzeros per stripe row on average
+  uint64_t cand[4], nH[4] = {0, 0, 0, 0}, nnzH[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 4; ++i) cand[i] = std::max<uint64_t>(8, nS << i);
+  for (uint32_t r = 0; r < nrows; ++r) {
+    const uint64_t len = rp[r + 1] - rp[r];
+    for (int i = 0; i < 4; ++i)
+      if (len >= cand[i]) {
+        ++nH[i];
+        nnzH[i] += len;
+      }
+  }
+  const uint64_t per_light = 4 + s + GATHER_BYTES;
+  const uint64_t none = per_light * nnz;
+  uint64_t best = none;
+  uint32_t thr = 0;
+  for (int i = 0; i < 4; ++i) {
+    if (nH[i] == 0) continue;
+    const uint64_t c = (2 + s) * nnzH[i] + (4 + 2 * s) * nS * nH[i] + per_light * (nnz - nnzH[i]);
+    if (c < best) {
+      best = c;
+      thr = (uint32_t)cand[i];
+    }
+  }
+  return best * 5 < none * 4 ? thr : 0;  // at least 20% less modelled traffic
+}
+
+// Builds the heavy part of a split plan (uploaded) and the light rows as host
+// CSR arrays (lrp without flags).  Leaves p->split.on false when no row is heavy.
+template <typename T>
+static int build_split(sparsep_plan *p, const typename Types<T>::csr *A, uint32_t thr, std::vector<uint32_t> &lrp,
+                       std::vector<uint32_t> &lci, std::vector<T> &lval, std::vector<uint32_t> &heavy) {
+  uint32_t W = 0, cap = 0, rcap = 0;
+  size_t smem = 0;
+  stripe_geometry<T>(&W, &smem, &cap, &rcap);
+  const uint32_t n = A->nrows;
+  const uint32_t *rp = A->rowptr;
+  heavy.clear();
+  for (uint32_t r = 0; r < n; ++r)
+    if (rp[r + 1] - rp[r] >= thr) heavy.push_back(r);
+  const uint64_t nH = heavy.size(), nS = ((uint64_t)A->ncols + W - 1) / W, V = nS * nH;
+  if (nH == 0 || V >= (1ull << 31) || V > 2 * (uint64_t)A->nnz + (1u << 20)) return SPARSEP_OK;
+  std::vector<uint32_t> vptr, cur;
+  std::vector<uint16_t> hcol;
+  std::vector<T> hval;
+  try {
+    vptr.assign(V + 1 + 8, 0);
+    for (uint64_t k = 0; k < nH; ++k) {
+      const uint32_t r = heavy[k];
+      for (uint32_t j = rp[r]; j < rp[r + 1]; ++j) ++vptr[(uint64_t)(A->colind[j] / W) * nH + k + 1];
+    }
+    for (uint64_t v = 0; v < V; ++v) vptr[v + 1] += vptr[v];
+    const uint64_t nnzH = vptr[V];
+    for (uint64_t v = V + 1; v < vptr.size(); ++v) vptr[v] = (uint32_t)nnzH;
+    hcol.assign(nnzH + 32, 0);
+    hval.assign(nnzH + 32, T(0));
+    cur.assign(vptr.begin(), vptr.begin() + V);
+    for (uint64_t k = 0; k < nH; ++k) {
+      const uint32_t r = heavy[k];
+      for (uint32_t j = rp[r]; j < rp[r + 1]; ++j) {
+        const uint32_t c = A->colind[j], s = c / W;
+        const uint32_t pos = cur[(uint64_t)s * nH + k]++;
+        hcol[pos] = (uint16_t)(c - s * W);
+        hval[pos] = A->values[j];
+      }
+    }
+    // the light rows (heavy rows keep zero length)
+    lrp.assign((size_t)n + 1, 0);
+    lci.clear();
+    lval.clear();
+    lci.reserve((size_t)A->nnz - nnzH);
+    lval.reserve((size_t)A->nnz - nnzH);
+    for (uint32_t r = 0; r < n; ++r) {
+      if (rp[r + 1] - rp[r] < thr)
+        for (uint32_t j = rp[r]; j < rp[r + 1]; ++j) {
+          lci.push_back(A->colind[j]);
+          lval.push_back(A->values[j]);
+        }
+      lrp[r + 1] = (uint32_t)lci.size();
+    }
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
+  }
+  // chunks: <= cap nonzeros and <= rcap stripe rows of one stripe; a stripe row
+  // longer than cap becomes a run of pieces
+  std::vector<StripeChunk> ch;
+  {
+    StripeChunk c{};
+    bool open = false;
+    auto close = [&]() {
+      if (open) ch.push_back(c);
+      open = false;
+    };
+    for (uint64_t v = 0; v < V; ++v) {
+      const uint32_t s = (uint32_t)(v / nH), a = vptr[v], b = vptr[v + 1];
+      if (b - a > cap) {
+        close();
+        for (uint32_t o = a; o < b; o += cap) {
+          StripeChunk q{};
+          q.n0 = o;
+          q.n1 = std::min<uint32_t>(b, o + cap);
+          q.v0 = (uint32_t)v;
+          q.v1 = (uint32_t)v + 1;
+          q.stripe = s;
+          q.piece = 4u | (o == a ? 1u : 0u) | (q.n1 == b ? 2u : 0u);
+          ch.push_back(q);
+        }
+        continue;
+      }
+      if (open && (c.stripe != s || c.n1 - c.n0 + (b - a) > cap || c.v1 - c.v0 >= rcap)) close();
+      if (!open) {
+        c = StripeChunk{};
+        c.n0 = c.n1 = a;
+        c.v0 = c.v1 = (uint32_t)v;
+        c.stripe = s;
+        open = true;
+      }
+      c.n1 = b;
+      c.v1 = (uint32_t)v + 1;
+    }
+    close();
+  }
+  // contiguous chunk ranges per CTA (one CTA per SM), balanced by nonzeros plus
+  // a per-row and per-chunk cost; pieces of one row stay on one CTA
+  const uint32_t nch = (uint32_t)ch.size();
+  const uint32_t C = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)p->sms, nch));
+  std::vector<uint64_t> pre(nch + 1, 0);
+  for (uint32_t i = 0; i < nch; ++i) pre[i + 1] = pre[i] + (ch[i].n1 - ch[i].n0) + 2ull * (ch[i].v1 - ch[i].v0) + 256;
+  std::vector<uint32_t> first(C + 1, 0);
+  for (uint32_t b = 1; b < C; ++b) {
+    const uint64_t target = pre[nch] * b / C;
+    uint32_t i = (uint32_t)(std::lower_bound(pre.begin(), pre.end(), target) - pre.begin());
+    i = std::max(i, first[b - 1]);
+    while (i < nch && ch[i].piece && !(ch[i].piece & 1u)) ++i;
+    first[b] = std::min(i, nch);
+  }
+  first[C] = nch;
+  // uploads
+  auto &S = p->split;
+  int st;
+  if ((st = upload(p, heavy.data(), nH, 4, 0, (const void **)&S.hrow))) return st;
+  if ((st = upload(p, vptr.data(), vptr.size(), 4, 0, (const void **)&S.vptr))) return st;
+  if ((st = upload(p, hcol.data(), hcol.size(), 2, 0, (const void **)&S.hcol))) return st;
+  if ((st = upload(p, hval.data(), hval.size(), sizeof(T), 0, &S.hval))) return st;
+  if ((st = upload(p, ch.data(), ch.size(), sizeof(StripeChunk), 0, (const void **)&S.chunks))) return st;
+  if ((st = upload(p, first.data(), first.size(), 4, 0, (const void **)&S.cta_first))) return st;
+  if ((st = dalloc(p, (V + 8) * sizeof(T), &S.part))) return st;
+  p->info.scratch_bytes += (V + 8) * sizeof(T);
+  S.on = true;
+  S.threshold = thr;
+  S.nH = (uint32_t)nH;
+  S.nS = (uint32_t)nS;
+  S.W = W;
+  S.ctas = C;
+  S.nchunks = nch;
+  S.nnz = vptr[V];
+  S.n_vptr = vptr.size();
+  S.n_h = hcol.size();
+  S.n_part = V;
+  return SPARSEP_OK;
+}
+
+// ---------------------------------------------------------------------------
 // CSR
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -527,9 +732,37 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
     else sparsep_partition_by_nnz(A->rowptr, A->nrows, oo.nr_parts, split.data());
     for (int i = 0; i < oo.nr_parts; ++i) csr_tile_items(items, t, A->rowptr, split[i], split[i + 1], oo, true, false);
   } else {
-    csr_tile_items(items, t, A->rowptr, 0, A->nrows, oo, false, true);
+    // a split plan when the heavy rows' x gathers are worth moving into
+    // shared-memory stripes (host arrays only: the re-layout reads columns)
+    std::vector<uint32_t> lrp, lci, heavy;
+    std::vector<T> lval;
+    const uint32_t *rp = A->rowptr;
+    if (!device_arrays && split_eligible(oo, A->nnz)) {
+      uint32_t W = 0;
+      stripe_geometry<T>(&W, nullptr, nullptr, nullptr);
+      const uint32_t thr = split_threshold(oo, A->rowptr, A->nrows, A->ncols, sizeof(T), W);
+      if (thr && (st = build_split<T>(p, A, thr, lrp, lci, lval, heavy))) return st;
+      if (p->split.on) rp = lrp.data();
+    }
+    csr_tile_items(items, t, rp, 0, A->nrows, oo, false, true);
     number_long_rows(items);
     for (auto &it : items) has_long |= it.kind == ITEM_LONG;
+    if (p->split.on) {
+      set_out_mode(p, oo, 1, has_long, 1);
+      for (const Item &it : items) p->max_item_nnz = std::max<uint32_t>(p->max_item_nnz, (uint32_t)(it.n1 - it.n0));
+      for (uint32_t r : heavy) lrp[r] |= 0x80000000u;  // rows the row kernels leave to the stripes
+      const uint64_t nl = lci.size();
+      if ((st = upload(p, lrp.data(), (size_t)A->nrows + 1, 4, 16, (const void **)&p->rowptr))) return st;
+      if ((st = upload(p, lci.data(), nl, 4, 16, (const void **)&p->colind))) return st;
+      if ((st = upload(p, lval.data(), nl, sizeof(T), 16, &p->val))) return st;
+      p->n_rowptr = (uint64_t)A->nrows + 17;
+      p->n_idx = p->n_val = nl + 16;
+      p->info.compulsory_bytes = compulsory_csr(A->nnz, A->nrows, A->ncols, sizeof(T));
+      if ((st = finish_plan(p, items, oo))) return st;
+      p->t[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      *out = guard.release();
+      return SPARSEP_OK;
+    }
   }
   set_out_mode(p, oo, 1, has_long, 1);
   p->pipe = !faithful && oo.lanes == 0 && p->out_mode == OUT_DIRECT && oo.pipeline == 1;
@@ -1326,6 +1559,29 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s, un
   P.n_carry = p->carry_w ? (uint64_t)p->nitems * p->carry_w + 1 : 0;
   P.nslots = p->out_mode == OUT_PARTIAL ? p->V : 1;
   P.smem_bytes = (uint32_t)p->smem;
+  if (p->split.on) {
+    // heavy rows first: stripes, then their merge into y; the row kernel then
+    // writes every other row (its band counters cover only its own rows)
+    const auto &S = p->split;
+    StripeParams<T> Q;
+    std::memset(&Q, 0, sizeof Q);
+    Q.chunks = S.chunks;
+    Q.cta_first = S.cta_first;
+    Q.vptr = S.vptr;
+    Q.hcol = S.hcol;
+    Q.hval = static_cast<const T *>(S.hval);
+    Q.x = static_cast<const T *>(d_x);
+    Q.part = static_cast<T *>(S.part);
+    Q.ncols = p->ncols;
+    Q.W = S.W;
+    Q.err = p->err;
+    Q.n_vptr = S.n_vptr;
+    Q.n_h = S.n_h;
+    Q.n_part = S.n_part;
+    CK(launch_stripes<T>(Q, S.ctas, s));
+    CK(launch_heavy_merge<T>(static_cast<const T *>(S.part), S.hrow, S.nH, S.nS, static_cast<T *>(d_y), p->sms, s));
+    P.row_flags = 1;
+  }
   if (p->pipe) CK(launch_csr_pipe<T>(P, p->sms, s, &p->pipe_grid, p->max_item_nnz));
   else CK(launch_items<T>(P, p->format, p->carry_w, p->threads, p->smem, s));
   if (p->out_mode == OUT_PARTIAL) {
