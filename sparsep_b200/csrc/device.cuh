@@ -180,22 +180,23 @@ template <typename T> struct Params {
   // array extents, used by the bounds-checked build (-DSPARSEP_CHECK)
   uint64_t n_rowptr, n_idx, n_val, n_elems, n_x, n_xalloc, n_carry;
   uint32_t nslots, smem_bytes;
-  // 1: bit 31 of a rowptr entry marks a row whose y belongs to the stripe
-  // path (a heavy row of a split CSR plan); the row kernels leave it alone
-  uint32_t row_flags;
 };
 
 // ---------------------------------------------------------------------------
-// Heavy rows of a split CSR plan, in column stripes (csr_stripes.cu).
-// The heavy rows (nH of them) are re-laid out stripe-major: stripe row
-// v = s * nH + k holds the nonzeros of heavy row k whose columns fall in
-// stripe s (columns [s*W, s*W + W)), with 16-bit stripe-local columns.  Its
-// sum is the partial part[v]; y[hrow[k]] = sum over s of part[s*nH + k].
+// Split CSR plans (csr_stripes.cu).  The heavy rows (nH of them) are laid out
+// stripe-major: stripe row v = s * nH + k holds the nonzeros of heavy row k
+// whose columns fall in stripe s (columns [s*W, s*W + W)), with 16-bit
+// stripe-local columns; its sum is the partial part[v], and
+// y[hrow[k]] = sum over s of part[s*nH + k].  The light rows stay a CSR
+// (heavy rows empty there) whose chunks write y directly.
 // ---------------------------------------------------------------------------
+constexpr uint32_t STRIPE_LIGHT = 0xFFFFFFFFu;  // StripeChunk::stripe of a light chunk
+constexpr uint32_t SPLIT_WARPS = 31;            // consumer warps of the split kernel (one more produces)
+
 struct StripeChunk {
-  uint32_t n0, n1;  // nonzeros [n0, n1) of the stripe-major arrays
-  uint32_t v0, v1;  // stripe rows [v0, v1); a piece of one long row has v1 = v0 + 1
-  uint32_t stripe;  // x columns [stripe * W, stripe * W + W)
+  uint32_t n0, n1;  // nonzeros [n0, n1) of the heavy (stripe-major) or light arrays
+  uint32_t v0, v1;  // stripe rows (heavy) or rows (light) [v0, v1); a piece has v1 = v0 + 1
+  uint32_t stripe;  // x columns [stripe * W, stripe * W + W); STRIPE_LIGHT for light rows
   uint32_t piece;   // 0: whole rows; a piece of row v0 has bit 2 set, bit 0 on its
                     // first piece and bit 1 on its last
 };
@@ -203,14 +204,19 @@ struct StripeChunk {
 template <typename T> struct StripeParams {
   const StripeChunk *chunks;
   const uint32_t *cta_first;  // chunks [cta_first[b], cta_first[b+1]) run on CTA b, in order
-  const uint32_t *vptr;       // nS * nH + 1 offsets into hcol / hval
-  const uint16_t *hcol;       // stripe-local columns
+  const uint16_t *wsplit;     // per chunk 32 row boundaries: consumer warp w takes rows [w, w+1)
+  const uint32_t *vptr;       // heavy: nS * nH + 1 offsets into hcol / hval
+  const uint16_t *hcol;       // heavy: stripe-local columns
   const T *hval;
+  const uint32_t *lptr;       // light: nrows + 1 offsets into lcol / lval
+  const uint32_t *lcol;
+  const T *lval;
   const T *x;
+  T *y;
   T *part;                    // nS * nH partial sums
-  uint32_t ncols, W;
+  uint32_t ncols, nrows, W;
   int *err;
-  uint64_t n_vptr, n_h, n_part;  // allocated extents (checked build)
+  uint64_t n_vptr, n_h, n_lptr, n_l, n_part;  // allocated extents (checked build)
 };
 
 // Bounds checks of the checked build: a failed check records `code` in the

@@ -21,12 +21,13 @@ cudaError_t launch_merge(const T *part, T *y, uint32_t nrows, uint32_t V, int sm
 template <typename T>
 cudaError_t launch_csr_pipe(const Params<T> &P, int sms, cudaStream_t st, int *grid_out, uint32_t max_item_nnz);
 
-// Heavy rows of a split CSR plan (csr_stripes.cu).  stripe_geometry gives the
-// stripe width (columns) and the dynamic shared memory of the stripe kernel
-// for element type T; launch_stripes runs `ctas` CTAs over the chunk lists;
+// Split CSR plans (csr_stripes.cu).  stripe_geometry gives, for element type
+// T, the stripe width (columns), the kernel's dynamic shared memory, the
+// nonzeros of a heavy and of a light chunk and the rows of a chunk;
+// launch_stripes runs `ctas` persistent CTAs over their chunk lists;
 // launch_heavy_merge writes y[hrow[k]] = sum over stripes of the partials.
 template <typename T>
-void stripe_geometry(uint32_t *width, size_t *smem, uint32_t *chunk_nnz, uint32_t *chunk_rows);
+void stripe_geometry(uint32_t *width, size_t *smem, uint32_t *chunk_nnz, uint32_t *light_nnz, uint32_t *chunk_rows);
 template <typename T>
 cudaError_t launch_stripes(const StripeParams<T> &P, uint32_t ctas, cudaStream_t st);
 template <typename T>

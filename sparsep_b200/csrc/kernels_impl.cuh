@@ -174,28 +174,15 @@ __device__ void csr_stream(const Params<T> &P, const Item &it, const T *__restri
   __shared__ uint32_t longs[CSR_RCAP];
   __shared__ uint32_t nlong;
   __shared__ A red[32];
-  __shared__ uint32_t skip[CSR_RCAP / 32 + 2];  // row_flags: rows left to the stripe path
   T *out = out_base(P, it);
   const uint32_t *rp = P.rowptr + it.ptr_base;
   const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool staged = it.xw > 0;
-  auto skipped = [&](uint32_t i) { return P.row_flags && ((skip[i >> 5] >> (i & 31)) & 1u); };
   uint64_t r = it.a0;
   while (r < it.a1) {
     const uint32_t nr = (uint32_t)((it.a1 - r) < CSR_RCAP ? (it.a1 - r) : CSR_RCAP);
     if (SP_BAD(P, it.ptr_base + r + nr < P.n_rowptr, -1001)) return;
-    if (P.row_flags) {
-      // bit 31 of a row's start marks a heavy row: kept as one bit per row
-      for (uint32_t i0 = (uint32_t)warp * 32; i0 <= nr; i0 += blockDim.x) {
-        const uint32_t i = i0 + lane;
-        const uint32_t v = i <= nr ? __ldcs(rp + r + i) : 0u;
-        if (i <= nr) srp[i] = v & 0x7FFFFFFFu;
-        const unsigned b = __ballot_sync(0xffffffffu, (v >> 31) != 0u);
-        if (lane == 0) skip[i0 >> 5] = b;
-      }
-    } else {
-      for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) srp[i] = __ldcs(rp + r + i);
-    }
+    for (uint32_t i = threadIdx.x; i <= nr; i += blockDim.x) srp[i] = __ldcs(rp + r + i);
     if (threadIdx.x == 0) nlong = 0;
     __syncthreads();
     // rows [r, r+k) form the chunk: the longest prefix within CSR_CAP nonzeros
@@ -211,7 +198,7 @@ __device__ void csr_stream(const Params<T> &P, const Item &it, const T *__restri
     }
     if (k == 0) {  // one row longer than the chunk: whole-CTA reduction from global
       const A tot = cta_range_sum<T>(P, it, xb, (uint64_t)base + it.nnz_base, (uint64_t)srp[1] + it.nnz_base, red);
-      if (threadIdx.x == 0 && !skipped(0)) put<T>(P, out, it.row_off + r, tot);
+      if (threadIdx.x == 0) put<T>(P, out, it.row_off + r, tot);
       __syncthreads();
       r += 1;
       continue;
@@ -237,7 +224,7 @@ __device__ void csr_stream(const Params<T> &P, const Item &it, const T *__restri
       if (b - a <= (uint32_t)CSR_SHORT) {
         A acc = A(0);
         for (uint32_t q = a; q < b; ++q) acc += prods[q];
-        if (!skipped(i)) put<T>(P, out, it.row_off + r + i, acc);
+        put<T>(P, out, it.row_off + r + i, acc);
       } else {
         longs[atomicAdd(&nlong, 1u)] = i;
       }
@@ -250,7 +237,7 @@ __device__ void csr_stream(const Params<T> &P, const Item &it, const T *__restri
       for (uint32_t q = a + lane; q < b; q += 32) acc += prods[q];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0 && !skipped(i)) put<T>(P, out, it.row_off + r + i, acc);
+      if (lane == 0) put<T>(P, out, it.row_off + r + i, acc);
     }
     __syncthreads();
     r += k;

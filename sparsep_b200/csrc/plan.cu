@@ -76,20 +76,21 @@ struct sparsep_plan {
   cudaEvent_t ev[5] = {};
   double t[5] = {0, 0, 0, 0, 0};
   sparsep_plan_info info{};
-  // Split 1D CSR plan: rows with >= `threshold` nonzeros (the heavy rows) run
-  // stripe-major in column stripes of W columns (csr_stripes.cu); the row
-  // kernels see the other rows only (rowptr, colind, val above hold them, with
-  // bit 31 of a heavy row's rowptr entry set).
+  // Split 1D CSR plan (csr_stripes.cu): rows with >= `threshold` nonzeros (the
+  // heavy rows) run stripe-major in column stripes of W columns; rowptr,
+  // colind and val above hold the other rows (the heavy ones empty).  One
+  // persistent kernel runs both, then a merge kernel sums the heavy rows'
+  // stripe partials into y.
   struct Split {
     bool on = false;
     uint32_t threshold = 0, nH = 0, nS = 0, W = 0, ctas = 0, nchunks = 0;
     uint64_t nnz = 0;  // heavy nonzeros
     const uint32_t *hrow = nullptr, *vptr = nullptr, *cta_first = nullptr;
-    const uint16_t *hcol = nullptr;
+    const uint16_t *hcol = nullptr, *wsplit = nullptr;
     const void *hval = nullptr;
     const StripeChunk *chunks = nullptr;
     void *part = nullptr;
-    uint64_t n_vptr = 0, n_h = 0, n_part = 0;
+    uint64_t n_vptr = 0, n_h = 0, n_lptr = 0, n_l = 0, n_part = 0;
   } split;
 };
 
@@ -437,7 +438,7 @@ static int finish_plan(sparsep_plan *p, std::vector<Item> &items, const sparsep_
   p->info.nblocks = p->nblocks;
   p->info.items = p->nitems;
   p->info.device_bytes += p->info.scratch_bytes;
-  p->info.kernel_launches = 1 + (p->out_mode == OUT_PARTIAL ? 1 : 0) + (p->split.on ? 2 : 0);
+  p->info.kernel_launches = p->split.on ? 2 : 1 + (p->out_mode == OUT_PARTIAL ? 1 : 0);
   p->info.workers = workers;
   p->info.stage_x = p->stage ? 1 : 0;
   p->info.y_bands = (int32_t)p->nbands;
@@ -564,25 +565,87 @@ static uint32_t split_threshold(const sparsep_opts &o, const uint32_t *rp, uint3
   return best * 5 < none * 4 ? thr : 0;  // at least 20% less modelled traffic
 }
 
-// Builds the heavy part of a split plan (uploaded) and the light rows as host
-// CSR arrays (lrp without flags).  Leaves p->split.on false when no row is heavy.
+// Chunks of one CSR-like array set: rows [0, nrows) of offsets `ptr`, cut at
+// `cap` nonzeros or `rcap` rows (and at stripe boundaries: rows v with
+// v / stripe_rows different); a row longer than `cap` becomes a run of pieces.
+static void cut_chunks(std::vector<StripeChunk> &ch, const std::vector<uint32_t> &ptr, uint64_t nrows, uint32_t cap,
+                       uint32_t rcap, uint64_t stripe_rows, bool light) {
+  StripeChunk c{};
+  bool open = false;
+  auto close = [&]() {
+    if (open) ch.push_back(c);
+    open = false;
+  };
+  for (uint64_t v = 0; v < nrows; ++v) {
+    const uint32_t s = light ? STRIPE_LIGHT : (uint32_t)(v / stripe_rows), a = ptr[v], b = ptr[v + 1];
+    if (b - a > cap) {
+      close();
+      for (uint32_t o = a; o < b; o += cap) {
+        StripeChunk q{};
+        q.n0 = o;
+        q.n1 = std::min<uint32_t>(b, o + cap);
+        q.v0 = (uint32_t)v;
+        q.v1 = (uint32_t)v + 1;
+        q.stripe = s;
+        q.piece = 4u | (o == a ? 1u : 0u) | (q.n1 == b ? 2u : 0u);
+        ch.push_back(q);
+      }
+      continue;
+    }
+    if (open && (c.stripe != s || c.n1 - c.n0 + (b - a) > cap || c.v1 - c.v0 >= rcap)) close();
+    if (!open) {
+      c = StripeChunk{};
+      c.n0 = c.n1 = a;
+      c.v0 = c.v1 = (uint32_t)v;
+      c.stripe = s;
+      open = true;
+    }
+    c.n1 = b;
+    c.v1 = (uint32_t)v + 1;
+  }
+  close();
+}
+
+// Cuts a chunk list into C contiguous ranges of about equal cost (nonzeros
+// times `per_nnz`, plus rows and a fixed cost per chunk); pieces of one row
+// stay in one range.  Returns C + 1 boundaries.
+static std::vector<uint32_t> cost_ranges(const std::vector<StripeChunk> &ch, uint32_t C, uint64_t per_nnz) {
+  const uint32_t n = (uint32_t)ch.size();
+  std::vector<uint64_t> pre(n + 1, 0);
+  for (uint32_t i = 0; i < n; ++i)
+    pre[i + 1] = pre[i] + per_nnz * (ch[i].n1 - ch[i].n0) + 2ull * (ch[i].v1 - ch[i].v0) + 256;
+  std::vector<uint32_t> first(C + 1, 0);
+  for (uint32_t b = 1; b < C; ++b) {
+    uint32_t i = (uint32_t)(std::lower_bound(pre.begin(), pre.end(), pre[n] * b / C) - pre.begin());
+    i = std::max(i, first[b - 1]);
+    while (i < n && ch[i].piece && !(ch[i].piece & 1u)) ++i;
+    first[b] = std::min(i, n);
+  }
+  first[C] = n;
+  return first;
+}
+
+// Builds a split plan's device arrays: the heavy rows (length >= thr) laid out
+// stripe-major, the light rows as a CSR (heavy rows empty), and per CTA one
+// chunk list interleaving its share of both.  Leaves p->split.on false when no
+// row is heavy or the stripe rows would outnumber the nonzeros.
 template <typename T>
-static int build_split(sparsep_plan *p, const typename Types<T>::csr *A, uint32_t thr, std::vector<uint32_t> &lrp,
-                       std::vector<uint32_t> &lci, std::vector<T> &lval, std::vector<uint32_t> &heavy) {
-  uint32_t W = 0, cap = 0, rcap = 0;
-  size_t smem = 0;
-  stripe_geometry<T>(&W, &smem, &cap, &rcap);
+static int build_split(sparsep_plan *p, const typename Types<T>::csr *A, uint32_t thr) {
+  uint32_t W = 0, cap = 0, cap_l = 0, rcap = 0;
+  stripe_geometry<T>(&W, nullptr, &cap, &cap_l, &rcap);
   const uint32_t n = A->nrows;
   const uint32_t *rp = A->rowptr;
-  heavy.clear();
+  std::vector<uint32_t> heavy;
   for (uint32_t r = 0; r < n; ++r)
     if (rp[r + 1] - rp[r] >= thr) heavy.push_back(r);
   const uint64_t nH = heavy.size(), nS = ((uint64_t)A->ncols + W - 1) / W, V = nS * nH;
   if (nH == 0 || V >= (1ull << 31) || V > 2 * (uint64_t)A->nnz + (1u << 20)) return SPARSEP_OK;
-  std::vector<uint32_t> vptr, cur;
+  std::vector<uint32_t> vptr, cur, lptr, lcol;
   std::vector<uint16_t> hcol;
-  std::vector<T> hval;
+  std::vector<T> hval, lval;
+  std::vector<StripeChunk> hch, lch, ch;
   try {
+    // heavy rows, stripe-major (counting sort of each row's nonzeros by stripe)
     vptr.assign(V + 1 + 8, 0);
     for (uint64_t k = 0; k < nH; ++k) {
       const uint32_t r = heavy[k];
@@ -603,84 +666,81 @@ static int build_split(sparsep_plan *p, const typename Types<T>::csr *A, uint32_
         hval[pos] = A->values[j];
       }
     }
-    // the light rows (heavy rows keep zero length)
-    lrp.assign((size_t)n + 1, 0);
-    lci.clear();
-    lval.clear();
-    lci.reserve((size_t)A->nnz - nnzH);
-    lval.reserve((size_t)A->nnz - nnzH);
+    // light rows, a CSR over all rows with the heavy ones empty
+    const uint64_t nnzL = (uint64_t)A->nnz - nnzH;
+    lptr.assign((size_t)n + 1 + 8, 0);
+    lcol.reserve(nnzL + 32);
+    lval.reserve(nnzL + 32);
     for (uint32_t r = 0; r < n; ++r) {
       if (rp[r + 1] - rp[r] < thr)
         for (uint32_t j = rp[r]; j < rp[r + 1]; ++j) {
-          lci.push_back(A->colind[j]);
+          lcol.push_back(A->colind[j]);
           lval.push_back(A->values[j]);
         }
-      lrp[r + 1] = (uint32_t)lci.size();
+      lptr[r + 1] = (uint32_t)lcol.size();
     }
+    for (size_t i = (size_t)n + 1; i < lptr.size(); ++i) lptr[i] = (uint32_t)nnzL;
+    lcol.resize(nnzL + 32, 0);
+    lval.resize(nnzL + 32, T(0));
+    cut_chunks(hch, vptr, V, cap, rcap, nH, false);
+    cut_chunks(lch, lptr, n, cap_l, rcap, 1, true);
   } catch (const std::bad_alloc &) {
     return SPARSEP_ENOMEM;
   }
-  // chunks: <= cap nonzeros and <= rcap stripe rows of one stripe; a stripe row
-  // longer than cap becomes a run of pieces
-  std::vector<StripeChunk> ch;
-  {
-    StripeChunk c{};
-    bool open = false;
-    auto close = [&]() {
-      if (open) ch.push_back(c);
-      open = false;
-    };
-    for (uint64_t v = 0; v < V; ++v) {
-      const uint32_t s = (uint32_t)(v / nH), a = vptr[v], b = vptr[v + 1];
-      if (b - a > cap) {
-        close();
-        for (uint32_t o = a; o < b; o += cap) {
-          StripeChunk q{};
-          q.n0 = o;
-          q.n1 = std::min<uint32_t>(b, o + cap);
-          q.v0 = (uint32_t)v;
-          q.v1 = (uint32_t)v + 1;
-          q.stripe = s;
-          q.piece = 4u | (o == a ? 1u : 0u) | (q.n1 == b ? 2u : 0u);
-          ch.push_back(q);
-        }
-        continue;
-      }
-      if (open && (c.stripe != s || c.n1 - c.n0 + (b - a) > cap || c.v1 - c.v0 >= rcap)) close();
-      if (!open) {
-        c = StripeChunk{};
-        c.n0 = c.n1 = a;
-        c.v0 = c.v1 = (uint32_t)v;
-        c.stripe = s;
-        open = true;
-      }
-      c.n1 = b;
-      c.v1 = (uint32_t)v + 1;
-    }
-    close();
-  }
-  // contiguous chunk ranges per CTA (one CTA per SM), balanced by nonzeros plus
-  // a per-row and per-chunk cost; pieces of one row stay on one CTA
-  const uint32_t nch = (uint32_t)ch.size();
-  const uint32_t C = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)p->sms, nch));
-  std::vector<uint64_t> pre(nch + 1, 0);
-  for (uint32_t i = 0; i < nch; ++i) pre[i + 1] = pre[i] + (ch[i].n1 - ch[i].n0) + 2ull * (ch[i].v1 - ch[i].v0) + 256;
+  // per CTA (one per SM): a contiguous share of the heavy chunks and one of the
+  // light chunks, interleaved by progress through each share, so that light
+  // gathers and heavy streaming overlap on every SM
+  const uint32_t C = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)p->sms, hch.size() + lch.size()));
+  const std::vector<uint32_t> fh = cost_ranges(hch, C, 1), fl = cost_ranges(lch, C, 3);
   std::vector<uint32_t> first(C + 1, 0);
-  for (uint32_t b = 1; b < C; ++b) {
-    const uint64_t target = pre[nch] * b / C;
-    uint32_t i = (uint32_t)(std::lower_bound(pre.begin(), pre.end(), target) - pre.begin());
-    i = std::max(i, first[b - 1]);
-    while (i < nch && ch[i].piece && !(ch[i].piece & 1u)) ++i;
-    first[b] = std::min(i, nch);
+  try {
+    ch.reserve(hch.size() + lch.size());
+    for (uint32_t b = 0; b < C; ++b) {
+      first[b] = (uint32_t)ch.size();
+      const uint64_t th = fh[b + 1] - fh[b], tl = fl[b + 1] - fl[b];
+      uint32_t i = fh[b], j = fl[b];
+      while (i < fh[b + 1] || j < fl[b + 1]) {
+        const bool h = j >= fl[b + 1] || (i < fh[b + 1] && (uint64_t)(i - fh[b]) * tl <= (uint64_t)(j - fl[b]) * th);
+        ch.push_back(h ? hch[i++] : lch[j++]);
+      }
+    }
+    first[C] = (uint32_t)ch.size();
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
   }
-  first[C] = nch;
-  // uploads
+  // each chunk's rows split over the consumer warps: warp w takes the rows
+  // whose first nonzero lies in [n*w/NW, n*(w+1)/NW) of the chunk's n nonzeros
+  constexpr uint32_t NW = SPLIT_WARPS;
+  std::vector<uint16_t> wsplit;
+  try {
+    wsplit.assign(ch.size() * (NW + 1), 0);
+  } catch (const std::bad_alloc &) {
+    return SPARSEP_ENOMEM;
+  }
+  for (size_t i = 0; i < ch.size(); ++i) {
+    const StripeChunk &c = ch[i];
+    uint16_t *w = wsplit.data() + i * (NW + 1);
+    const uint32_t nr = c.v1 - c.v0, nn = c.n1 - c.n0;
+    w[NW] = (uint16_t)nr;
+    if (c.piece) continue;
+    const uint32_t *pt = (c.stripe == STRIPE_LIGHT ? lptr.data() : vptr.data()) + c.v0;
+    uint32_t r = 0;
+    for (uint32_t q = 1; q < NW; ++q) {
+      const uint32_t t = (uint32_t)((uint64_t)nn * q / NW);
+      while (r < nr && pt[r] - c.n0 < t) ++r;
+      w[q] = (uint16_t)r;
+    }
+  }
   auto &S = p->split;
   int st;
+  if ((st = upload(p, wsplit.data(), wsplit.size(), 2, 0, (const void **)&S.wsplit))) return st;
   if ((st = upload(p, heavy.data(), nH, 4, 0, (const void **)&S.hrow))) return st;
   if ((st = upload(p, vptr.data(), vptr.size(), 4, 0, (const void **)&S.vptr))) return st;
   if ((st = upload(p, hcol.data(), hcol.size(), 2, 0, (const void **)&S.hcol))) return st;
   if ((st = upload(p, hval.data(), hval.size(), sizeof(T), 0, &S.hval))) return st;
+  if ((st = upload(p, lptr.data(), lptr.size(), 4, 0, (const void **)&p->rowptr))) return st;
+  if ((st = upload(p, lcol.data(), lcol.size(), 4, 0, (const void **)&p->colind))) return st;
+  if ((st = upload(p, lval.data(), lval.size(), sizeof(T), 0, &p->val))) return st;
   if ((st = upload(p, ch.data(), ch.size(), sizeof(StripeChunk), 0, (const void **)&S.chunks))) return st;
   if ((st = upload(p, first.data(), first.size(), 4, 0, (const void **)&S.cta_first))) return st;
   if ((st = dalloc(p, (V + 8) * sizeof(T), &S.part))) return st;
@@ -691,10 +751,12 @@ static int build_split(sparsep_plan *p, const typename Types<T>::csr *A, uint32_
   S.nS = (uint32_t)nS;
   S.W = W;
   S.ctas = C;
-  S.nchunks = nch;
+  S.nchunks = (uint32_t)ch.size();
   S.nnz = vptr[V];
   S.n_vptr = vptr.size();
   S.n_h = hcol.size();
+  S.n_lptr = lptr.size();
+  S.n_l = lcol.size();
   S.n_part = V;
   return SPARSEP_OK;
 }
@@ -734,35 +796,23 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
   } else {
     // a split plan when the heavy rows' x gathers are worth moving into
     // shared-memory stripes (host arrays only: the re-layout reads columns)
-    std::vector<uint32_t> lrp, lci, heavy;
-    std::vector<T> lval;
-    const uint32_t *rp = A->rowptr;
     if (!device_arrays && split_eligible(oo, A->nnz)) {
       uint32_t W = 0;
-      stripe_geometry<T>(&W, nullptr, nullptr, nullptr);
+      stripe_geometry<T>(&W, nullptr, nullptr, nullptr, nullptr);
       const uint32_t thr = split_threshold(oo, A->rowptr, A->nrows, A->ncols, sizeof(T), W);
-      if (thr && (st = build_split<T>(p, A, thr, lrp, lci, lval, heavy))) return st;
-      if (p->split.on) rp = lrp.data();
+      if (thr && (st = build_split<T>(p, A, thr))) return st;
+      if (p->split.on) {  // no row items: one persistent kernel runs both parts
+        set_out_mode(p, oo, 1, false, 1);
+        p->info.compulsory_bytes = compulsory_csr(A->nnz, A->nrows, A->ncols, sizeof(T));
+        if ((st = finish_plan(p, items, oo))) return st;
+        p->t[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        *out = guard.release();
+        return SPARSEP_OK;
+      }
     }
-    csr_tile_items(items, t, rp, 0, A->nrows, oo, false, true);
+    csr_tile_items(items, t, A->rowptr, 0, A->nrows, oo, false, true);
     number_long_rows(items);
     for (auto &it : items) has_long |= it.kind == ITEM_LONG;
-    if (p->split.on) {
-      set_out_mode(p, oo, 1, has_long, 1);
-      for (const Item &it : items) p->max_item_nnz = std::max<uint32_t>(p->max_item_nnz, (uint32_t)(it.n1 - it.n0));
-      for (uint32_t r : heavy) lrp[r] |= 0x80000000u;  // rows the row kernels leave to the stripes
-      const uint64_t nl = lci.size();
-      if ((st = upload(p, lrp.data(), (size_t)A->nrows + 1, 4, 16, (const void **)&p->rowptr))) return st;
-      if ((st = upload(p, lci.data(), nl, 4, 16, (const void **)&p->colind))) return st;
-      if ((st = upload(p, lval.data(), nl, sizeof(T), 16, &p->val))) return st;
-      p->n_rowptr = (uint64_t)A->nrows + 17;
-      p->n_idx = p->n_val = nl + 16;
-      p->info.compulsory_bytes = compulsory_csr(A->nnz, A->nrows, A->ncols, sizeof(T));
-      if ((st = finish_plan(p, items, oo))) return st;
-      p->t[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      *out = guard.release();
-      return SPARSEP_OK;
-    }
   }
   set_out_mode(p, oo, 1, has_long, 1);
   p->pipe = !faithful && oo.lanes == 0 && p->out_mode == OUT_DIRECT && oo.pipeline == 1;
@@ -1560,27 +1610,35 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s, un
   P.nslots = p->out_mode == OUT_PARTIAL ? p->V : 1;
   P.smem_bytes = (uint32_t)p->smem;
   if (p->split.on) {
-    // heavy rows first: stripes, then their merge into y; the row kernel then
-    // writes every other row (its band counters cover only its own rows)
+    // one persistent kernel over the heavy stripes and the light rows, then
+    // the heavy rows' stripe partials summed into y
     const auto &S = p->split;
     StripeParams<T> Q;
     std::memset(&Q, 0, sizeof Q);
     Q.chunks = S.chunks;
     Q.cta_first = S.cta_first;
+    Q.wsplit = S.wsplit;
     Q.vptr = S.vptr;
     Q.hcol = S.hcol;
     Q.hval = static_cast<const T *>(S.hval);
+    Q.lptr = p->rowptr;
+    Q.lcol = p->colind;
+    Q.lval = static_cast<const T *>(p->val);
     Q.x = static_cast<const T *>(d_x);
+    Q.y = static_cast<T *>(d_y);
     Q.part = static_cast<T *>(S.part);
     Q.ncols = p->ncols;
+    Q.nrows = p->nrows;
     Q.W = S.W;
     Q.err = p->err;
     Q.n_vptr = S.n_vptr;
     Q.n_h = S.n_h;
+    Q.n_lptr = S.n_lptr;
+    Q.n_l = S.n_l;
     Q.n_part = S.n_part;
     CK(launch_stripes<T>(Q, S.ctas, s));
     CK(launch_heavy_merge<T>(static_cast<const T *>(S.part), S.hrow, S.nH, S.nS, static_cast<T *>(d_y), p->sms, s));
-    P.row_flags = 1;
+    return SPARSEP_OK;
   }
   if (p->pipe) CK(launch_csr_pipe<T>(P, p->sms, s, &p->pipe_grid, p->max_item_nnz));
   else CK(launch_items<T>(P, p->format, p->carry_w, p->threads, p->smem, s));
