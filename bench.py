@@ -13,9 +13,23 @@ scaling).  `e2e` is the same metric through sparsep_execute_host: pinned host
 x in, pinned host y out, copies inside the timed region.  `clocks` is sampled
 through NVML every millisecond during the timed region.
 
-`batched` (one GPU): the batched multi-RHS path on 512 matrices -- plain
-per-matrix launches against the one-launch work queue with the default,
-learned (sparsep_batch_select) and exhaustively autotuned variants.
+`batched` / `batched_i32` (one GPU): the batched multi-RHS path on 512
+matrices, FP32 and INT32 -- plain per-matrix launches against the one-launch
+work queue with the default, learned (sparsep_batch_select) and exhaustively
+autotuned variants, a sample checked against the reference's host SpMV.
+
+`configs` (one GPU): every other configuration of the workload list -- the
+4096-row uniform INT32 CSR; the Zipf matrix in FP32 / FP64 as CSR and COO, 1D
+with auto items, row / nnz balance over 2048 parts, lock-free and atomic, and
+2D equal (D), equal-width (RBD) and variable (BD) tilings; the 2M-row
+block-banded matrix as BCSR / BCOO 4x4 and 8x8 in INT8 / INT16 / INT64 /
+FP32, block and nnz balance over 2048 parts.  Each entry: device time (L2
+flushed), GB/s of compulsory bytes, fraction of the measured HBM copy
+bandwidth, the reference's host SpMV for that kind on one core, and the check
+against its result (integers bit-exact, FP within 2 gamma_n sum|a x|).
+
+The headline run is gated: its y must match the reference's host SpMV within
+that bound, or the run fails.
 
 --impl reference times the reference's own host SpMV (spmv_host of
 spmv/1D/CSR-row/host/app.c, compiled from the reference sources into
@@ -183,10 +197,10 @@ def run_ours(args, rank, world):
     sh = stream.cuda_stream
     launches_per_step = int(info.kernel_launches)
 
-    # correctness gate on the benchmark matrix: FP32 bound vs the high-precision oracle
-    sys.path.insert(0, str(ROOT / "tests"))
+    # one untimed run; its y is checked in the CPU-baseline leg below
     plan.run_device(xd.data_ptr(), yd.data_ptr(), sh)
     torch.cuda.synchronize()
+    y_first = yd.cpu().numpy()
 
     for _ in range(args.warmup):
         flush.zero_()
@@ -232,6 +246,15 @@ def run_ours(args, rank, world):
     e2e_avg = max_over_ranks(sum(e2e_ms) / len(e2e_ms), world, "cuda")
     y_dev = yd.cpu().numpy()
     assert np.array_equal(y_dev, hy.numpy()), "device and host paths disagree"
+    # the same calls back to back, without the L2 flush and device
+    # synchronisation in front of each (what those add to the spread)
+    e2e_bb = []
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        sp.capi.check(lib.sparsep_execute_host(plan.h, C.c_void_p(hx.data_ptr()), C.c_void_p(hy.data_ptr())))
+        e2e_bb.append((time.perf_counter() - t1) * 1e3)
+    link = link_probe(hx, xd, hy, yd, reps=20)
 
     # the gather floor: x read at this matrix's column indices and nothing else
     ci_d = torch.from_numpy(colind[:nnz].view(np.int32)).cuda()
@@ -278,6 +301,9 @@ def run_ours(args, rank, world):
                 "ms_quantiles": {q: round(float(np.quantile(e2e_ms, f)), 4)
                                  for q, f in (("min", 0.0), ("p50", 0.5), ("p90", 0.9), ("max", 1.0))},
                 "y_bands": int(info.y_bands),
+                "back_to_back_ms_quantiles": {q: round(float(np.quantile(e2e_bb, f)), 4)
+                                              for q, f in (("min", 0.0), ("p50", 0.5), ("max", 1.0))},
+                "link_probe": link,
                 "phases_ms": {"load_input_vector": round(float(phases[1]), 4), "kernel": round(float(phases[2]), 4),
                               "retrieve_output_vector": round(float(phases[3]), 4),
                               "merge": round(float(phases[4]), 4), "load_matrix_once": round(load_ms, 3),
@@ -289,27 +315,65 @@ def run_ours(args, rank, world):
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
-        res["cpu_baseline"] = cpu_baseline(n, m, rowptr, colind, values, x, budget_s=args.cpu_budget,
-                                           threads=1)
+        res["cpu_baseline"], y_ref, y_abs = cpu_baseline(n, m, rowptr, colind, values, x,
+                                                         budget_s=args.cpu_budget, threads=1)
+        # the correctness gate: the benchmark's y (first run and last timed
+        # run) against the reference's own host SpMV on the same matrix and x,
+        # within 2 gamma_n sum|a x| per row; a failure ends the run
+        counts = np.diff(rowptr.astype(np.int64))
+        ok1, r1 = fp_check(y_first, y_ref, y_abs, counts, "f32")
+        ok2, r2 = fp_check(y_dev, y_ref, y_abs, counts, "f32")
+        res["check"] = {"ok": ok1 and ok2, "max_err_over_bound": round(max(r1, r2), 4),
+                        "against": f"spmv_host of spmv/1D/CSR-row/host/app.c ({res['cpu_baseline']['kind']}), "
+                                   "per row |y - y_ref| <= 2 gamma_n sum|a x|"}
+        if not (ok1 and ok2):
+            raise SystemExit(f"correctness gate failed: max err / bound = {max(r1, r2):.3g}")
     plan.free()
     return res
 
 
-def run_batch(args):
-    """The batched multi-RHS path (FP32) on the 512-matrix workload: plain
-    per-matrix launches (default variant per matrix) against the one-launch
-    queue with the default, learned and exhaustively autotuned variants.
-    The batch's compulsory bytes (8.9 GB) exceed L2 many times over, so no
-    flush is needed between timed runs."""
+def link_probe(hx, xd, hy, yd, reps=20):
+    """Host<->device copy rates of this box's link: the x and y sizes of the
+    benchmark, pinned host memory, one copy per direction per rep on the
+    current stream, device-timed; median GB/s of each direction."""
+    import torch
+
+    st = torch.cuda.current_stream()
+    out = {}
+    for name, dst, src in (("h2d", xd, hx), ("d2h", hy, yd)):
+        ts = []
+        for i in range(reps + 3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            dst.copy_(src, non_blocking=True)
+            e1.record(st)
+            torch.cuda.synchronize()
+            if i >= 3:
+                ts.append(e0.elapsed_time(e1))
+        ms = statistics.median(ts)
+        out[name] = {"bytes": int(src.numel() * src.element_size()), "ms": round(ms, 4),
+                     "gbs": round(src.numel() * src.element_size() / (ms * 1e-3) / 1e9, 2)}
+    return out
+
+
+def run_batch(args, dt="f32"):
+    """The batched multi-RHS path on the 512-matrix workload (FP32 or INT32):
+    plain per-matrix launches (default variant per matrix) against the
+    one-launch queue with the default, learned and exhaustively autotuned
+    variants.  The batch's compulsory bytes (8.9 GB) exceed L2 many times over,
+    so no flush is needed between timed runs.  A sample of matrices is checked
+    column by column against the reference's CSR host SpMV (CPU-baseline leg:
+    integers bit-exact, FP32 within 2 gamma_n sum|a x|), which is also timed."""
     import torch
 
     import sparsep_b200 as sp
     from sparsep_b200 import capi, selector
 
     t0 = time.time()
-    w = sp.synth.batch_workload(nmats=args.batch_mats, dtype=np.float32)
-    mats = [sp.csr("f32", d["n"], d["n"], d["rowptr"], d["colind"], d["values"]) for d in w]
-    b = capi.Batch("f32", mats, [d["k"] for d in w])
+    npdt = capi.DTYPES[dt].np
+    w = sp.synth.batch_workload(nmats=args.batch_mats, dtype=npdt)
+    mats = [sp.csr(dt, d["n"], d["n"], d["rowptr"], d["colind"], d["values"]) for d in w]
+    b = capi.Batch(dt, mats, [d["k"] for d in w])
     for m, d in enumerate(w):
         b.set_x(m, d["x"])
     setup_s = time.time() - t0
@@ -341,30 +405,64 @@ def run_batch(args):
     select_s = time.time() - t0
     learned = timeit(lambda: b.execute(st.cuda_stream))
     b.status()
-    dev = max(float(np.abs(b.get_y(m) - y_plain[m]).max() / max(np.abs(y_plain[m]).max(), 1e-30)) for m in sample)
+    y_learned = {m: b.get_y(m) for m in sample}
     t0 = time.time()
     b.autotune(reps=3)
     tune_s = time.time() - t0
     tuned = timeit(lambda: b.execute(st.cuda_stream))
     b.status()
+    y_tuned = {m: b.get_y(m) for m in sample}
     b.free()
+
+    check = {"matrices": len(sample), "columns": 0, "ok": True, "max_err_over_bound": 0.0}
+    cpu_s, cpu_bytes = 0.0, 0
+    if not args.no_cpu_baseline:
+        ref = RefHost("csr", dt)
+        for m in sample:
+            d = w[m]
+            A = mats[m]
+            Aa = sp.csr(dt, d["n"], d["n"], d["rowptr"], d["colind"], np.abs(d["values"])) if dt == "f32" else None
+            counts = np.diff(d["rowptr"].astype(np.int64))
+            for j in sorted({0, d["k"] // 2, d["k"] - 1}):  # first, middle and last right-hand side
+                xj = np.ascontiguousarray(d["x"][:, j])
+                y_ref, sec = ref.run(A, xj)
+                cpu_s += sec
+                cpu_bytes += int(d["rowptr"][-1]) * 8 + (d["n"] + 1) * 4 + 2 * d["n"] * 4
+                y_abs = ref.run(Aa, np.abs(xj))[0] if Aa is not None else None
+                for y_all in (y_plain[m], y_learned[m], y_tuned[m]):
+                    y = y_all.reshape(d["n"], d["k"])[:, j]
+                    if y_abs is None:
+                        ok, r = bool(np.array_equal(y, y_ref)), 0.0
+                    else:
+                        ok, r = fp_check(y, y_ref, y_abs, counts, dt)
+                    check["ok"] &= ok
+                    check["max_err_over_bound"] = max(check["max_err_over_bound"], round(r, 4))
+                check["columns"] += 1
+        check["against"] = ("spmv_host of spmv/1D/CSR-row/host/app.c per right-hand side, for the plain, learned "
+                            "and autotuned runs: " + ("bit-exact" if dt != "f32" else "|y - y_ref| <= 2 gamma_n "
+                                                      "sum|a x| per row"))
 
     def gbs(ms):
         return round(cb / (ms * 1e-3) / 1e9, 2)
 
-    return {"workload": f"{len(w)} CSR matrices, rows log-uniform 1k-256k, uniform / Zipf / banded, 1-32 "
-                        "right-hand sides each, FP32 (seed 3)",
-            "nnz": int(info["nnz"]), "compulsory_bytes": int(cb), "items": int(info["items"]),
-            "plain_per_matrix_ms": round(plain, 3), "queue_default_ms": round(default, 3),
-            "queue_learned_ms": round(learned, 3), "queue_autotuned_ms": round(tuned, 3),
-            "learned_speedup_vs_plain": round(plain / learned, 3),
-            "learned_over_autotuned": round(learned / tuned, 4),
-            "gbs": {"plain": gbs(plain), "default": gbs(default), "learned": gbs(learned), "autotuned": gbs(tuned)},
-            "select_s": round(select_s, 3), "autotune_s": round(tune_s, 2), "setup_s": round(setup_s, 1),
-            "learned_max_rel_diff_vs_plain": dev,
-            "accuracy": "FP32 sums per row in a variant-dependent order; every variant is within the per-row "
-                        "gamma bound (tests); INT32 bit-exact",
-            "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
+    out = {"workload": f"{len(w)} CSR matrices, rows log-uniform 1k-256k, uniform / Zipf / banded, 1-32 "
+                       f"right-hand sides each, {dt.upper()} (seed 3)",
+           "dtype": dt, "nnz": int(info["nnz"]), "compulsory_bytes": int(cb), "items": int(info["items"]),
+           "plain_per_matrix_ms": round(plain, 3), "queue_default_ms": round(default, 3),
+           "queue_learned_ms": round(learned, 3), "queue_autotuned_ms": round(tuned, 3),
+           "learned_speedup_vs_plain": round(plain / learned, 3),
+           "learned_over_autotuned": round(learned / tuned, 4),
+           "gbs": {"plain": gbs(plain), "default": gbs(default), "learned": gbs(learned), "autotuned": gbs(tuned)},
+           "select_s": round(select_s, 3), "autotune_s": round(tune_s, 2), "setup_s": round(setup_s, 1),
+           "check": check,
+           "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
+    if cpu_s > 0:
+        out["cpu_baseline"] = {"value": round(cpu_bytes / cpu_s / 1e9, 3), "unit": "GB/s", "cores": 1,
+                               "kind": ref.kind, "sample": f"{check['columns']} single-vector passes of the "
+                               f"reference's CSR spmv_host over {len(sample)} of the matrices"}
+    log(f"[bench] batch {dt}: plain {plain:.2f} ms, learned {learned:.2f} ms, autotuned {tuned:.2f} ms, "
+        f"check {check}")
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -489,6 +587,90 @@ def measure_struct(cfg, workload, A, A_abs, x, counts, cases, peak, stream, flus
     return out
 
 
+PARTS = 2048  # parts of the reference's 2048-DPU runs: one part = one CTA
+
+
+def run_configs(args, peak):
+    """Every single-matrix configuration of the workload list, one entry per
+    format / scheme / balance / element type: device time, GB/s of compulsory
+    bytes, fraction of the measured HBM copy bandwidth, the reference's own
+    host SpMV for that kind on one core, and the check against it."""
+    import torch
+
+    import sparsep_b200 as sp
+    from sparsep_b200 import capi
+
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    out = []
+    t0 = time.time()
+
+    # 1: uniform 4096 x 4096, 8 columns per row, INT32, CSR 1D nnz-balanced
+    n, m, r, c, v, x = sp.synth.uniform_rows(4096, 4096, 8, 0, np.int32)
+    A = sp.csr("i32", n, m, *sp.synth.to_csr(n, r, c, v))
+    out += measure_struct(1, "uniform8-4096", A, None, x, None,
+                          [("1d auto", {}), ("1d nnz-balanced 64 parts", dict(nr_parts=64, part_balance=capi.BAL_NNZ))],
+                          peak, stream, flush)
+
+    # 2: the 1M-row Zipf matrix, FP32 and FP64, CSR and COO, 1D and 2D
+    for dt in ("f32", "f64"):
+        n, m, r, c, v, x = sp.synth.zipf_rows(seed=1, dtype=capi.DTYPES[dt].np)
+        counts = np.bincount(r.astype(np.int64), minlength=n)
+        rp, ci, vals = sp.synth.to_csr(n, r, c, v)
+        A, Aa = sp.csr(dt, n, m, rp, ci, vals), sp.csr(dt, n, m, rp, ci, np.abs(vals))
+        out += measure_struct(2, "zipf-1M", A, Aa, x, counts,
+                              [("1d auto", {}),
+                               ("1d row-balanced 2048 parts", dict(nr_parts=PARTS, part_balance=capi.BAL_ROW)),
+                               ("1d nnz-balanced 2048 parts",
+                                dict(nr_parts=PARTS, part_balance=capi.BAL_NNZ, worker_balance=capi.BAL_NNZ))],
+                              peak, stream, flush)
+        del A, Aa
+        E, Ea = sp.cooe(dt, n, m, r, c, v), sp.cooe(dt, n, m, r, c, np.abs(v))
+        out += measure_struct(2, "zipf-1M", E, Ea, x, counts,
+                              [("1d lock-free auto", {}), ("1d atomic", dict(sync=capi.SYNC_ATOMIC)),
+                               ("1d nnz-elem 2048 parts", dict(nr_parts=PARTS, part_balance=capi.BAL_NNZ_ELEM))],
+                              peak, stream, flush)
+        for conv, hv, cases in (("cooe2dcsr", (16, 16), [("2d-D 16x16", {})]),
+                                ("cooe2rbdcsr", (32, 32), [("2d-RBD 32x32", {})]),
+                                ("cooe2bdcsr", (64, 64), [("2d-BD 64x64", {}),
+                                                          ("2d-BD 64x64 atomic", dict(sync=capi.SYNC_ATOMIC))]),
+                                ("cooe2dcoo", (16, 16), [("2d-D 16x16", {}),
+                                                         ("2d-D 16x16 atomic", dict(sync=capi.SYNC_ATOMIC))]),
+                                ("cooe2bdcoo", (64, 64), [("2d-BD 64x64", {})])):
+            D, Da = sp.convert(conv, E, *hv), sp.convert(conv, Ea, *hv)
+            out += measure_struct(2, "zipf-1M", D, Da, x, counts, cases, peak, stream, flush)
+            del D, Da
+        del E, Ea
+    log(f"[bench] configs 1-2 in {time.time() - t0:.0f}s")
+
+    # 3: the 2M-row block-banded matrix, BCSR and BCOO 4x4 / 8x8, block and nnz balance
+    for rb in (4, 8):
+        for dt in ("i8", "i16", "i64", "f32"):
+            B = sp.synth.block_banded(rb=rb, cb=rb, dtype=capi.DTYPES[dt].np)
+            A = capi.bcsr(dt, B["nrows"], B["ncols"], rb, rb, B["browptr"], B["bcolind"], B["bval"], B["nnz"],
+                          B["nnz_per_block"])
+            O = sp.convert("bcsr2bcoo", A)
+            counts = Aa = Oa = None
+            if dt == "f32":
+                counts = np.repeat(np.diff(B["browptr"].astype(np.int64)) * rb, rb)[: B["nrows"]]
+                Aa = capi.bcsr(dt, B["nrows"], B["ncols"], rb, rb, B["browptr"], B["bcolind"], np.abs(B["bval"]),
+                               B["nnz"], B["nnz_per_block"])
+                Oa = sp.convert("bcsr2bcoo", Aa)
+            wl = f"banded-2M {rb}x{rb}"
+            out += measure_struct(3, wl, A, Aa, B["x"], counts,
+                                  [("1d block-balanced 2048 parts", dict(nr_parts=PARTS, part_balance=capi.BAL_BLOCK)),
+                                   ("1d nnz-balanced 2048 parts", dict(nr_parts=PARTS, part_balance=capi.BAL_NNZ))],
+                                  peak, stream, flush)
+            out += measure_struct(3, wl, O, Oa, B["x"], counts,
+                                  [("1d block-balanced 2048 parts", dict(nr_parts=PARTS, part_balance=capi.BAL_BLOCK)),
+                                   ("1d nnz-elem 2048 parts", dict(nr_parts=PARTS, part_balance=capi.BAL_NNZ_ELEM))],
+                                  peak, stream, flush)
+            del A, O, Aa, Oa, B
+    log(f"[bench] configs 1-3 in {time.time() - t0:.0f}s")
+    del flush
+    return out
+
+
 def _ref_csr_lib():
     so = ROOT / "oracle" / "_ref" / "libref_1D_CSR_row_f32.so"
     if so.exists():
@@ -500,11 +682,15 @@ def _ref_csr_lib():
 
 
 def cpu_baseline(n, m, rowptr, colind, values, x, budget_s=15.0, threads=1):
-    """Time the reference's host CSR SpMV on a bounded number of full passes."""
+    """Time the reference's host CSR SpMV on a bounded number of full passes;
+    also returns its y and its sum of |a||x| per row (the check's bound)."""
     import sparsep_b200 as sp
 
     L, kind = _ref_csr_lib()
     A = sp.csr("f32", n, m, rowptr, colind, values)
+    ref = RefHost("csr", "f32")
+    y_ref = ref.run(A, np.ascontiguousarray(x))[0]
+    y_abs = ref.run(sp.csr("f32", n, m, rowptr, colind, np.abs(values)), np.abs(x))[0]
     y = np.zeros(n + 8, np.float32)
     xx = np.ascontiguousarray(x)
     nnz = int(rowptr[-1])
@@ -529,7 +715,7 @@ def cpu_baseline(n, m, rowptr, colind, values, x, budget_s=15.0, threads=1):
     dt = (time.perf_counter() - t0) / reps
     return {"value": round(cb / dt / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
             "sample": f"{reps} full SpMV passes over the {n}-row matrix ({nnz} nnz), {dt * 1e3:.1f} ms each",
-            "ms_per_spmv": round(dt * 1e3, 3), "cpu": _cpu_name()}
+            "ms_per_spmv": round(dt * 1e3, 3), "cpu": _cpu_name()}, y_ref, y_abs
 
 
 def slices(L, kind, A, x, y, threads):
@@ -614,9 +800,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", default="all", choices=["all", "single", "batch"],
-                    help="single: the FP32 CSR Zipf SpMV only; batch: the batched path only")
+    ap.add_argument("--only", default="all", choices=["all", "single", "batch", "configs"],
+                    help="single: the FP32 CSR Zipf SpMV only; batch: the batched path only; configs: the "
+                         "per-configuration entries only")
     ap.add_argument("--batch-mats", type=int, default=512)
+    ap.add_argument("--no-configs", action="store_true",
+                    help="leave out the per-configuration entries (formats, schemes, element types)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -634,15 +823,29 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.impl == "reference":
         res = run_reference(args, rank, world)
+    elif args.only == "configs":
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        peak, _ = peaks()
+        res = None
+        if rank == 0:
+            cfg = run_configs(args, peak)
+            res = {"configs": cfg, "configs_checked": f"{sum(e['check_ok'] for e in cfg)}/{len(cfg)}"}
     elif args.only == "batch":
         import torch
 
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        res = {"batched": run_batch(args)} if rank == 0 else None
+        res = {"batched": run_batch(args, "f32"), "batched_i32": run_batch(args, "i32")} if rank == 0 else None
     else:
         res = run_ours(args, rank, world)
         if args.only == "all" and world == 1:
-            res["batched"] = run_batch(args)
+            res["batched"] = run_batch(args, "f32")
+            res["batched_i32"] = run_batch(args, "i32")
+            if not args.no_configs:
+                peak, _ = peaks()
+                res["configs"] = run_configs(args, peak)
+                res["configs_checked"] = f"{sum(e['check_ok'] for e in res['configs'])}/{len(res['configs'])}"
     if world > 1 and args.impl == "ours":
         import torch.distributed as dist
 

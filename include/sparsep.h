@@ -746,6 +746,24 @@ int sparsep_spmv_cooe_f32_noalloc(const sparsep_elem_f32 *d_elems, uint32_t nnz,
                                   const float *d_x, float *d_y, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Test support: failures on purpose, without faulting a GPU                 */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference (its failures abort, DPU_ASSERT in
+ * spmv/1D/CSR-row/host/app.c:91-93).  sparsep_test_fail_alloc(n): the n-th
+ * device allocation the library makes from now on fails as a full device
+ * would (the call returns SPARSEP_ENOMEM); 0 switches it off.
+ * sparsep_test_live_allocations: device allocations the library holds now
+ * (a call that failed must leave it unchanged).  sparsep_test_wait_fault(1):
+ * kernels with a bounded staging wait (2D tiles staging their x segment, the
+ * batched launch) add, after their own copies have landed, one wait that
+ * nothing completes; it runs out after 1024 tries and the call reports
+ * SPARSEP_ETIMEDOUT (the batch: sparsep_batch_status).  Nothing is left in
+ * flight, so the next call with the switch off succeeds. */
+int sparsep_test_fail_alloc(int nth);
+long long sparsep_test_live_allocations(void);
+int sparsep_test_wait_fault(int on);
+
+/* ------------------------------------------------------------------------ */
 /* Device information                                                        */
 /* ------------------------------------------------------------------------ */
 /* Number of SMs of the current device, or a negative status. */

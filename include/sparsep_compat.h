@@ -108,4 +108,59 @@ typedef int32_t val_dt;
 #define sparsep_csr2bcsr SPARSEP_FN(csr2bcsr)
 #define sparsep_bcsr2bcoo SPARSEP_FN(bcsr2bcoo)
 
+/*
+ * With -DSPARSEP_REFERENCE_NAMES, the reference's own reader, converter and
+ * free functions with its own signatures, so an unmodified host/app.c keeps
+ * its calls: pointer-returning as in spmv/1D/CSR-row/support/matrix.h:44
+ * (readCOOMatrix), :113 (coo2csr), :102 / :158 (freeCOOMatrix /
+ * freeCSRMatrix), spmv/1D/BCSR-nnz/support/matrix.h:202 (csr2bcsr), :515
+ * (freeBCSRMatrix), spmv/1D/BCOO-nnz/support/matrix.h:549 (bcsr2bcoo), :607
+ * (freeBCOOMatrix) and spmv/1D/COO-nnz/support/matrix.h:31 / :88
+ * (readCOOMatrix, sortCOOMatrix of the AoS layout).  readCOOMatrix pads
+ * nrows / ncols as the CSR-family reader does; -DSPARSEP_COO_NOPAD selects
+ * the BCSR / BCOO families' reader, which does not.  Where the reference
+ * aborts, these return NULL (the status is in sparsep_last_error /
+ * the status-returning forms above).
+ */
+#ifdef SPARSEP_REFERENCE_NAMES
+/* typed entry point of the selected element type, pasted directly (the
+   generic names above are macros themselves) */
+#define SPARSEP_TFN2(name, sfx) sparsep_##name##_##sfx
+#define SPARSEP_TFN1(name, sfx) SPARSEP_TFN2(name, sfx)
+#define SPARSEP_TFN(name) SPARSEP_TFN1(name, SPARSEP_SFX)
+#ifdef SPARSEP_COO_ELEM
+static inline struct COOMatrix *readCOOMatrix(const char *fileName) {
+  struct COOMatrix *A = NULL;
+  return SPARSEP_TFN(read_cooe)(fileName, &A) == SPARSEP_OK ? A : NULL;
+}
+static inline void sortCOOMatrix(struct COOMatrix *A) { (void)SPARSEP_TFN(sort_cooe)(A); }
+static inline void freeCOOMatrix(struct COOMatrix *A) { SPARSEP_TFN(free_cooe)(A); }
+#else
+static inline struct COOMatrix *readCOOMatrix(const char *fileName) {
+  struct COOMatrix *A = NULL;
+#ifdef SPARSEP_COO_NOPAD
+  return SPARSEP_TFN(read_coo_nopad)(fileName, &A) == SPARSEP_OK ? A : NULL;
+#else
+  return SPARSEP_TFN(read_coo)(fileName, &A) == SPARSEP_OK ? A : NULL;
+#endif
+}
+static inline void freeCOOMatrix(struct COOMatrix *A) { SPARSEP_TFN(free_coo)(A); }
+static inline struct CSRMatrix *coo2csr(struct COOMatrix *B) {
+  struct CSRMatrix *A = NULL;
+  return SPARSEP_TFN(coo2csr)(B, &A) == SPARSEP_OK ? A : NULL;
+}
+#endif
+static inline void freeCSRMatrix(struct CSRMatrix *A) { SPARSEP_TFN(free_csr)(A); }
+static inline struct BCSRMatrix *csr2bcsr(struct CSRMatrix *A, uint32_t row_block_size, uint32_t col_block_size) {
+  struct BCSRMatrix *B = NULL;
+  return SPARSEP_TFN(csr2bcsr)(A, row_block_size, col_block_size, &B) == SPARSEP_OK ? B : NULL;
+}
+static inline void freeBCSRMatrix(struct BCSRMatrix *B) { SPARSEP_TFN(free_bcsr)(B); }
+static inline struct BCOOMatrix *bcsr2bcoo(struct BCSRMatrix *B) {
+  struct BCOOMatrix *O = NULL;
+  return SPARSEP_TFN(bcsr2bcoo)(B, &O) == SPARSEP_OK ? O : NULL;
+}
+static inline void freeBCOOMatrix(struct BCOOMatrix *O) { SPARSEP_TFN(free_bcoo)(O); }
+#endif /* SPARSEP_REFERENCE_NAMES */
+
 #endif /* SPARSEP_COMPAT_H_ */

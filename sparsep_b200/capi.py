@@ -175,6 +175,9 @@ def lib() -> C.CDLL:
     L.sparsep_version.restype = C.c_char_p
     L.sparsep_last_error.restype = C.c_char_p
     L.sparsep_opts_default.argtypes = [C.POINTER(Opts)]
+    L.sparsep_test_fail_alloc.argtypes = [C.c_int]
+    L.sparsep_test_live_allocations.restype = C.c_longlong
+    L.sparsep_test_wait_fault.argtypes = [C.c_int]
     L.sparsep_plan_free.argtypes = [C.c_void_p]
     L.sparsep_plan_get_info.argtypes = [C.c_void_p, C.POINTER(PlanInfo)]
     L.sparsep_timings.argtypes = [C.c_void_p, C.POINTER(C.c_double)]

@@ -12,6 +12,7 @@
 #include <thread>
 #include <vector>
 
+#include "fault.hpp"
 #include "batch.hpp"
 #include "internal.hpp"
 
@@ -63,7 +64,7 @@ static int bmap(cudaError_t e) {
 
 static int balloc(sparsep_batch *b, size_t bytes, void **out) {
   void *d = nullptr;
-  BCK(cudaMalloc(&d, bytes ? bytes : 16));
+  BCK(dev_malloc((void **)&d, bytes ? bytes : 16));
   b->allocs.push_back(d);
   *out = d;
   return SPARSEP_OK;
@@ -73,7 +74,7 @@ static void bfree(sparsep_batch *b, void *d) {
   if (!d) return;
   for (auto i = b->allocs.begin(); i != b->allocs.end(); ++i)
     if (*i == d) {
-      cudaFree(*i);
+      dev_free(*i);
       b->allocs.erase(i);
       return;
     }
@@ -325,6 +326,13 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
   return SPARSEP_OK;
 }
 
+// err[1] carries the test-support wait fault to the kernel (read on the device,
+// so a captured graph sees the switch as it is at launch)
+static int set_fault_word(sparsep_batch *b, cudaStream_t s) {
+  BCK(cudaMemsetAsync(b->err + 1, wait_fault() ? 1 : 0, sizeof(int), s));
+  return SPARSEP_OK;
+}
+
 template <typename T>
 static int launch_queue(sparsep_batch *b, cudaStream_t s) {
   if (b->ticket) BCK(cudaMemsetAsync(b->head, 0, 4, s));
@@ -368,7 +376,7 @@ void sparsep_batch_free(sparsep_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  for (void *d : b->allocs) cudaFree(d);
+  for (void *d : b->allocs) dev_free(d);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -425,6 +433,7 @@ int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y) {
 int sparsep_batch_execute(sparsep_batch *b, void *stream) {
   if (!b) return SPARSEP_EINVAL;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  if (int st = set_fault_word(b, s)) return st;
   if (!b->exec) {
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int st = dispatch_queue(b, b->stream);
@@ -449,6 +458,7 @@ int sparsep_batch_execute(sparsep_batch *b, void *stream) {
 int sparsep_batch_execute_per_matrix(sparsep_batch *b, void *stream) {
   if (!b) return SPARSEP_EINVAL;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  if (int st = set_fault_word(b, s)) return st;
   for (uint32_t m = 0; m < b->nmats; ++m)
     if (int st = dispatch_items(b, b->base_d, b->base0[m], b->nbase[m], s)) return st;
   if (stream) return SPARSEP_OK;
@@ -523,7 +533,7 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
   *us_out = 0.0;
   if (items.empty()) return SPARSEP_OK;
   BItem *d = nullptr;
-  BCK(cudaMalloc(&d, items.size() * sizeof(BItem)));
+  BCK(dev_malloc((void **)&d, items.size() * sizeof(BItem)));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   // same stream as the timed launches: the items are in place before the first
   int st = bmap(cudaMemcpyAsync(d, items.data(), items.size() * sizeof(BItem), cudaMemcpyHostToDevice, b->stream));
@@ -539,7 +549,7 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
-  cudaFree(d);
+  dev_free(d);
   if (st) return st;
   std::sort(ms.begin(), ms.end());
   *us_out = 1e3 * ms[ms.size() / 2];

@@ -183,6 +183,14 @@ __device__ __forceinline__ bool landed(uint64_t *bar, uint32_t parity, int *err)
     spin();
     return false;
   }
+  // test support: err[1] set (sparsep_test_wait_fault) adds a wait that runs
+  // out once the copies above have landed; the item is then given up as on a
+  // real timeout
+  if (err && *reinterpret_cast<volatile int *>(err + 1)) {
+    uint32_t ph = parity ^ 1u;
+    inject_wait_timeout(bar, ph, err);
+    return false;
+  }
   return true;
 }
 

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <new>
 
+#include "fault.hpp"
 #include "internal.hpp"
 #include "sparsep.h"
 
@@ -307,11 +308,11 @@ int sparsep_cg_create(sparsep_plan *plan, sparsep_cg **out) {
   c->n = info.nrows;
   c->esize = info.dtype == SPARSEP_FP32 ? 4 : 8;
   const size_t vb = (c->n + 64) * c->esize;
-  int st = cg_err(cudaMalloc(&c->r, vb));
-  if (!st) st = cg_err(cudaMalloc(&c->p, vb));
-  if (!st) st = cg_err(cudaMalloc(&c->q, vb));
-  if (!st) st = cg_err(cudaMalloc(&c->part, sizeof(double) * NB));
-  if (!st) st = cg_err(cudaMalloc(&c->sc, sizeof(double) * S_NSC));
+  int st = cg_err(sparsep::dev_malloc((void **)&c->r, vb));
+  if (!st) st = cg_err(sparsep::dev_malloc((void **)&c->p, vb));
+  if (!st) st = cg_err(sparsep::dev_malloc((void **)&c->q, vb));
+  if (!st) st = cg_err(sparsep::dev_malloc((void **)&c->part, sizeof(double) * NB));
+  if (!st) st = cg_err(sparsep::dev_malloc((void **)&c->sc, sizeof(double) * S_NSC));
   if (!st) st = cg_err(cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking));
   if (st) {
     sparsep_cg_free(c);
@@ -326,7 +327,7 @@ void sparsep_cg_free(sparsep_cg *c) {
   if (c->exec) cudaGraphExecDestroy(c->exec);
   if (c->graph) cudaGraphDestroy(c->graph);
   for (void *d : {c->r, c->p, c->q, (void *)c->part, (void *)c->sc})
-    if (d) cudaFree(d);
+    if (d) sparsep::dev_free(d);
   if (c->cap) cudaStreamDestroy(c->cap);
   delete c;
 }
@@ -354,9 +355,9 @@ int sparsep_power_create(sparsep_plan *plan, sparsep_power **out) {
   w->dtype = info.dtype;
   w->n = info.nrows;
   const size_t es = info.dtype == SPARSEP_FP32 ? 4 : 8;
-  int st = cg_err(cudaMalloc(&w->q, (w->n + 64) * es));
-  if (!st) st = cg_err(cudaMalloc(&w->part, sizeof(double) * NB));
-  if (!st) st = cg_err(cudaMalloc(&w->sc, sizeof(double) * S_NSC));
+  int st = cg_err(sparsep::dev_malloc((void **)&w->q, (w->n + 64) * es));
+  if (!st) st = cg_err(sparsep::dev_malloc((void **)&w->part, sizeof(double) * NB));
+  if (!st) st = cg_err(sparsep::dev_malloc((void **)&w->sc, sizeof(double) * S_NSC));
   if (!st) st = cg_err(cudaMemset(w->sc, 0, sizeof(double) * S_NSC));
   if (!st) st = cg_err(cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking));
   if (st) {
@@ -372,7 +373,7 @@ void sparsep_power_free(sparsep_power *w) {
   if (w->exec) cudaGraphExecDestroy(w->exec);
   if (w->graph) cudaGraphDestroy(w->graph);
   for (void *d : {w->q, (void *)w->part, (void *)w->sc})
-    if (d) cudaFree(d);
+    if (d) sparsep::dev_free(d);
   if (w->cap) cudaStreamDestroy(w->cap);
   delete w;
 }

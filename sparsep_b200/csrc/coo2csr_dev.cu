@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <new>
 
+#include "fault.hpp"
 #include "internal.hpp"
 #include "radix.cuh"
 #include "sparsep.h"
@@ -67,11 +68,11 @@ static int coo2csr_device(const uint32_t *rows, const uint32_t *cols, const void
   uint32_t *buf = nullptr;
   int *bad = nullptr;
   const size_t words = 2 * (size_t)nnz + sparsep::radix::radix_scratch_words(nnz);
-  int st = c2c_err(cudaMalloc(&buf, words * 4));
-  if (!st) st = c2c_err(cudaMalloc(&bad, sizeof(int)));
+  int st = c2c_err(sparsep::dev_malloc((void **)&buf, words * 4));
+  if (!st) st = c2c_err(sparsep::dev_malloc((void **)&bad, sizeof(int)));
   if (st) {
-    cudaFree(buf);
-    cudaFree(bad);
+    sparsep::dev_free(buf);
+    sparsep::dev_free(bad);
     return st;
   }
   const uint32_t *key = nullptr, *idx = nullptr;
@@ -99,8 +100,8 @@ static int coo2csr_device(const uint32_t *rows, const uint32_t *cols, const void
     st = c2c_err(cudaGetLastError());
     if (!st) st = c2c_err(cudaStreamSynchronize(s));
   }
-  cudaFree(buf);
-  cudaFree(bad);
+  sparsep::dev_free(buf);
+  sparsep::dev_free(bad);
   return st;
 }
 

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <new>
 
+#include "fault.hpp"
 #include "internal.hpp"
 #include "radix.cuh"
 #include "sparsep.h"
@@ -168,7 +169,7 @@ static int layout(const uint32_t *rowptr, const uint32_t *colind, uint32_t nrows
   const int bits = L->jbits + bits_for(L->nbr);
   int *bad = nullptr;
   uint32_t *dnb = nullptr;
-  int st = c2b_err(cudaMalloc(&bad, 2 * sizeof(int)));
+  int st = c2b_err(sparsep::dev_malloc((void **)&bad, 2 * sizeof(int)));
   if (st) return st;
   dnb = reinterpret_cast<uint32_t *>(bad + 1);
   int h_bad = 0;
@@ -183,8 +184,8 @@ static int layout(const uint32_t *rowptr, const uint32_t *colind, uint32_t nrows
     const size_t rsw = radix_scratch_words(nnz);
     const size_t words = 6 * (size_t)nnz + rsw + ((size_t)nnz + nbs + 8) + ((size_t)nnz + 1) + 8;
     uint32_t *buf = nullptr;
-    st = c2b_err(cudaMalloc(&buf, words * 4));
-    if (!st) st = c2b_err(cudaMalloc(&L->row, (size_t)nnz * 4));
+    st = c2b_err(sparsep::dev_malloc((void **)&buf, words * 4));
+    if (!st) st = c2b_err(sparsep::dev_malloc((void **)&L->row, (size_t)nnz * 4));
     if (!st) {
       uint64_t *key = reinterpret_cast<uint64_t *>(buf), *k0 = key + nnz, *k1 = k0 + nnz;
       uint32_t *scratch = reinterpret_cast<uint32_t *>(k1 + nnz);
@@ -206,23 +207,23 @@ static int layout(const uint32_t *rowptr, const uint32_t *colind, uint32_t nrows
       if (!st) st = c2b_err(cudaMemcpyAsync(&L->nblocks, dnb, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       if (!st) st = c2b_err(cudaStreamSynchronize(s));
       if (!st && h_bad) st = SPARSEP_EINVAL;
-      if (!st) st = c2b_err(cudaMalloc(&L->sidx, (size_t)nnz * 4));
-      if (!st) st = c2b_err(cudaMalloc(&L->bstart, ((size_t)L->nblocks + 1) * 4));
-      if (!st) st = c2b_err(cudaMalloc(&L->bkey, (size_t)std::max<uint32_t>(L->nblocks, 1) * 8));
+      if (!st) st = c2b_err(sparsep::dev_malloc((void **)&L->sidx, (size_t)nnz * 4));
+      if (!st) st = c2b_err(sparsep::dev_malloc((void **)&L->bstart, ((size_t)L->nblocks + 1) * 4));
+      if (!st) st = c2b_err(sparsep::dev_malloc((void **)&L->bkey, (size_t)std::max<uint32_t>(L->nblocks, 1) * 8));
       if (!st) st = c2b_err(cudaMemcpyAsync(L->sidx, sidx, (size_t)nnz * 4, cudaMemcpyDeviceToDevice, s));
       if (!st)
         st = c2b_err(cudaMemcpyAsync(L->bstart, bstart_tmp, ((size_t)L->nblocks + 1) * 4, cudaMemcpyDeviceToDevice, s));
       if (!st) st = c2b_err(cudaMemcpyAsync(L->bkey, bkey_tmp, (size_t)L->nblocks * 8, cudaMemcpyDeviceToDevice, s));
       if (!st) st = c2b_err(cudaStreamSynchronize(s));
     }
-    cudaFree(buf);
+    sparsep::dev_free(buf);
   } else if (!st) {
     st = c2b_err(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (!st) st = c2b_err(cudaStreamSynchronize(s));
     if (!st && h_bad) st = SPARSEP_EINVAL;
     L->nblocks = 0;
   }
-  cudaFree(bad);
+  sparsep::dev_free(bad);
   return st;
 }
 
@@ -262,7 +263,7 @@ int sparsep_bcsr_layout_device(const uint32_t *d_rowptr, const uint32_t *d_colin
 void sparsep_bcsr_layout_free(sparsep_bcsr_layout *L) {
   if (!L) return;
   for (void *d : {(void *)L->row, (void *)L->sidx, (void *)L->bstart, (void *)L->bkey})
-    if (d) cudaFree(d);
+    if (d) sparsep::dev_free(d);
   delete L;
 }
 

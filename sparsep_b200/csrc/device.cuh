@@ -180,6 +180,7 @@ template <typename T> struct Params {
   // array extents, used by the bounds-checked build (-DSPARSEP_CHECK)
   uint64_t n_rowptr, n_idx, n_val, n_elems, n_x, n_xalloc, n_carry;
   uint32_t nslots, smem_bytes;
+  int fault_wait;  // test support: add a staging wait that nothing completes (after the copy)
 };
 
 // ---------------------------------------------------------------------------
@@ -246,9 +247,34 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
+// Test support (sparsep_test_wait_fault): once the CTA's own copies have
+// landed, thread 0 arms one more phase of `mbar` for 16 bytes that no copy
+// brings; the CTA's bounded wait on it (1024 tries) runs out and records
+// SPARSEP_ETIMEDOUT, then thread 0 completes the phase itself, so the barrier
+// is left clean and nothing is in flight.
+__device__ __forceinline__ void inject_wait_timeout(uint64_t *mbar, uint32_t &phase, int *err) {
+  __syncthreads();
+  if (threadIdx.x == 0)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(16u)
+                 : "memory");
+  uint32_t done = 0;
+  for (uint32_t it = 0; it < (1u << 10) && !done; ++it) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(mbar)), "r"(phase)
+        : "memory");
+  }
+  if (!__syncthreads_or(done) && threadIdx.x == 0 && err) atomicExch(err, SPARSEP_ETIMEDOUT);
+  if (threadIdx.x == 0)
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(16u) : "memory");
+  __syncthreads();
+  phase ^= 1u;
+}
+
 template <typename T>
 __device__ const T *stage_x(const T *x, uint32_t lo, uint32_t w, unsigned char *smem, uint64_t *mbar,
-                            uint32_t &phase, int *err, uint32_t smem_cap, uintptr_t x_end) {
+                            uint32_t &phase, int *err, uint32_t smem_cap, uintptr_t x_end, int fault = 0) {
   (void)smem_cap;
   (void)x_end;
   uintptr_t gb = reinterpret_cast<uintptr_t>(x) + (uintptr_t)lo * sizeof(T);
@@ -288,6 +314,7 @@ __device__ const T *stage_x(const T *x, uint32_t lo, uint32_t w, unsigned char *
   }
   if (!done && err) atomicExch(err, SPARSEP_ETIMEDOUT);
   phase ^= 1u;
+  if (fault && done) inject_wait_timeout(mbar, phase, err);
   return reinterpret_cast<const T *>(smem + (gb - g0)) - lo;
 }
 

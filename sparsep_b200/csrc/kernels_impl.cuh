@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(512) spmv_items(Params<T> P, uint32_t carry_w)
     uint32_t phase = 0;
     mbar_init(&mbar);
     xb = stage_x<T>(P.x, it.xlo, it.xw, dyn_smem, &mbar, phase, P.err, P.smem_bytes,
-                    reinterpret_cast<uintptr_t>(P.x + P.n_xalloc));
+                    reinterpret_cast<uintptr_t>(P.x + P.n_xalloc), P.fault_wait);
   }
 
   if constexpr (FMT == SPARSEP_FMT_CSR) {

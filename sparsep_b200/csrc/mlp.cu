@@ -30,6 +30,7 @@
 #include <cstdio>
 #include <new>
 
+#include "fault.hpp"
 #include "internal.hpp"
 #include "sparsep.h"
 
@@ -295,7 +296,7 @@ int sparsep_selector_create(const uint16_t *wb, const float *feat_mean, const fl
     s->mean[i] = feat_mean[i];
     s->stdev[i] = feat_std[i] > 0.f ? feat_std[i] : 1.f;
   }
-  int st = map_err(cudaMalloc(&s->wb, sizeof(__nv_bfloat16) * NP));
+  int st = map_err(sparsep::dev_malloc((void **)&s->wb, sizeof(__nv_bfloat16) * NP));
   if (!st) st = map_err(cudaMemcpy(s->wb, wb, sizeof(__nv_bfloat16) * NP, cudaMemcpyHostToDevice));
   if (st) {
     sparsep_selector_free(s);
@@ -307,7 +308,7 @@ int sparsep_selector_create(const uint16_t *wb, const float *feat_mean, const fl
 
 void sparsep_selector_free(sparsep_selector *s) {
   if (!s) return;
-  if (s->wb) cudaFree(s->wb);
+  if (s->wb) sparsep::dev_free(s->wb);
   delete s;
 }
 
@@ -324,14 +325,14 @@ int sparsep_selector_scores(sparsep_selector *s, const float *feats, uint32_t n,
   }
   for (size_t q = 0; q < (size_t)n * F; ++q) hx[q] = (feats[q] - s->mean[q % F]) / s->stdev[q % F];
   float *dx = nullptr, *dl = nullptr;
-  int st = map_err(cudaMalloc(&dx, sizeof(float) * n * F));
-  if (!st) st = map_err(cudaMalloc(&dl, sizeof(float) * n * K));
+  int st = map_err(sparsep::dev_malloc((void **)&dx, sizeof(float) * n * F));
+  if (!st) st = map_err(sparsep::dev_malloc((void **)&dl, sizeof(float) * n * K));
   if (!st) st = map_err(cudaMemcpy(dx, hx, sizeof(float) * n * F, cudaMemcpyHostToDevice));
   if (!st) st = sparsep_mlp_forward(reinterpret_cast<const uint16_t *>(s->wb), dx, n, dl, nullptr);
   if (!st) st = map_err(cudaMemcpy(logits, dl, sizeof(float) * n * K, cudaMemcpyDeviceToHost));
   delete[] hx;
-  if (dx) cudaFree(dx);
-  if (dl) cudaFree(dl);
+  if (dx) sparsep::dev_free(dx);
+  if (dl) sparsep::dev_free(dl);
   return st;
 }
 

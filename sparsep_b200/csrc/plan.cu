@@ -22,6 +22,7 @@
 
 #include <cuda.h>
 
+#include "fault.hpp"
 #include "internal.hpp"
 #include "kernels.hpp"
 
@@ -126,7 +127,7 @@ static size_t dtype_size(int d) {
 static int dalloc(sparsep_plan *p, size_t bytes, void **out) {
   void *d = nullptr;
   if (bytes == 0) bytes = 16;
-  CK(cudaMalloc(&d, bytes));
+  CK(dev_malloc((void **)&d, bytes));
   p->allocs.push_back(d);
   // on the plan's stream: finish_plan waits for it, so every later launch,
   // on any stream, sees the buffer complete
@@ -1609,6 +1610,7 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s, un
   P.n_carry = p->carry_w ? (uint64_t)p->nitems * p->carry_w + 1 : 0;
   P.nslots = p->out_mode == OUT_PARTIAL ? p->V : 1;
   P.smem_bytes = (uint32_t)p->smem;
+  P.fault_wait = wait_fault();
   if (p->split.on) {
     // one persistent kernel over the heavy stripes and the light rows, then
     // the heavy rows' stripe partials summed into y
@@ -1685,14 +1687,14 @@ static int plan_csr_device(uint32_t nrows, uint32_t ncols, uint32_t nnz, const u
   CK(cudaMemcpy(rp.data(), d_rowptr, rp.size() * 4, cudaMemcpyDeviceToHost));
   if (nnz) {
     int *bad = nullptr, h = 0;
-    CK(cudaMalloc(&bad, sizeof(int)));
+    CK(dev_malloc((void **)&bad, sizeof(int)));
     cudaError_t e = cudaMemset(bad, 0, sizeof(int));
     if (e == cudaSuccess) {
       cols_in_range<<<std::min<uint64_t>(4096, (nnz + 255) / 256), 256>>>(d_colind, nnz, ncols, bad);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(&h, bad, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(bad);
+    dev_free(bad);
     CK(e);
     if (h) return SPARSEP_EINVAL;
   }
@@ -1731,14 +1733,14 @@ static int plan_bcsr_device(uint32_t nrows, uint32_t ncols, uint32_t rb, uint32_
     if (bp[i] > bp[i + 1]) return SPARSEP_EINVAL;
   if (nblocks) {
     int *bad = nullptr, h = 0;
-    CK(cudaMalloc(&bad, sizeof(int)));
+    CK(dev_malloc((void **)&bad, sizeof(int)));
     cudaError_t e = cudaMemset(bad, 0, sizeof(int));
     if (e == cudaSuccess) {
       cols_in_range<<<std::min<uint64_t>(4096, (nblocks + 255) / 256), 256>>>(d_bcolind, nblocks, nbc, bad);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(&h, bad, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(bad);
+    dev_free(bad);
     CK(e);
     if (h) return SPARSEP_EINVAL;
   }
@@ -1820,7 +1822,7 @@ void sparsep_plan_free(sparsep_plan *p) {
     cudaStreamSynchronize(p->copy_stream);
     cudaStreamDestroy(p->copy_stream);
   }
-  for (void *d : p->allocs) cudaFree(d);
+  for (void *d : p->allocs) dev_free(d);
   if (p->h_err) cudaFreeHost(p->h_err);
   for (auto &e : p->ev)
     if (e) cudaEventDestroy(e);

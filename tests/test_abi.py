@@ -109,6 +109,19 @@ def test_compat_header_builds_reference_style_code(tmp_path, macro):
     assert r.returncode == 0, r.stderr
 
 
+@pytest.mark.parametrize("macro", ["INT8", "INT16", "INT32", "INT64", "FP32", "FP64"])
+def test_reference_names_build(tmp_path, macro):
+    """An unmodified-style reference host program that calls readCOOMatrix,
+    coo2csr, csr2bcsr, bcsr2bcoo and free*Matrix by the reference's own names
+    and signatures (tests/ref_app.c, -DSPARSEP_REFERENCE_NAMES) compiles
+    warning-free and links to the library; tests/test_gpu_c_programs.py runs it."""
+    out = tmp_path / "ref_app"
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", f"-I{ROOT / 'include'}",
+                        "-DSPARSEP_REFERENCE_NAMES", f"-D{macro}", str(ROOT / "tests" / "ref_app.c"),
+                        f"-L{ROOT / 'sparsep_b200'}", "-lsparsep_b200", "-o", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_api_example_builds(tmp_path):
     """A C caller of the batch, selector, CG and value-reader entry points
     (tests/api_example.c) compiles warning-free and links to the library."""
