@@ -746,6 +746,34 @@ int sparsep_spmv_cooe_f32_noalloc(const sparsep_elem_f32 *d_elems, uint32_t nnz,
                                   const float *d_x, float *d_y, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Plan variants of a CSR matrix (sparsep_opts.autotune; no reference        */
+/* counterpart: there each choice is a separate program)                    */
+/* ------------------------------------------------------------------------ */
+/* A CSR input can run as any of SPARSEP_NPLANVARIANTS plans -- CSR auto items,
+ * CSR 2048-nonzero items, the CSR TMA pipeline, the heavy-row stripes, COO
+ * lock-free, COO atomic, BCSR 4x4, BCSR 8x8, BCOO 4x4, 2D equal-tile COO
+ * 16x16 atomic -- all computing the same y (integers bit-exact, FP within the
+ * per-row gamma bound).  sparsep_plan_csr_<t> with o->autotune = 2 times every
+ * applicable one (block formats need a block fill >= 1/4; the stripes an x of
+ * at least 1 MB) and keeps the fastest; autotune = 1 lets the learned selector
+ * (the MLP of the batch selector, trained on these timings) pick, falling back
+ * to timing when its confidence is below one half.  The plan's info.variant
+ * names the choice.  autotune applies to 1D CSR inputs with one right-hand
+ * side on host arrays (ENOSYS otherwise). */
+#define SPARSEP_NPLANVARIANTS 10
+const char *sparsep_plan_variant_name(int v);
+/* every variant timed (median of reps after a warm-up, device x and y), us;
+ * 0 where a variant does not apply; best receives the fastest's index */
+#define SPARSEP_DECLARE_AUTOTUNE(T, S) \
+  int sparsep_plan_autotune_csr_##S(const sparsep_csr_##S *A, int reps, double *times_us, int32_t *best);
+SPARSEP_DECLARE_AUTOTUNE(int8_t, i8)
+SPARSEP_DECLARE_AUTOTUNE(int16_t, i16)
+SPARSEP_DECLARE_AUTOTUNE(int32_t, i32)
+SPARSEP_DECLARE_AUTOTUNE(int64_t, i64)
+SPARSEP_DECLARE_AUTOTUNE(float, f32)
+SPARSEP_DECLARE_AUTOTUNE(double, f64)
+
+/* ------------------------------------------------------------------------ */
 /* Test support: failures on purpose, without faulting a GPU                 */
 /* ------------------------------------------------------------------------ */
 /* No counterpart in the reference (its failures abort, DPU_ASSERT in

@@ -394,9 +394,12 @@ class Plan:
         return int(self.info.ncols)
 
     def run_host(self, x: np.ndarray) -> np.ndarray:
+        """y = A x on host buffers; with nrhs = k > 1, x is ncols x k and y
+        nrows x k (row-major)."""
+        k = max(1, int(self.info.nrhs))
         x = np.ascontiguousarray(x, dtype=self.dt.np)
-        assert x.size >= self.ncols
-        y = np.zeros(self.nrows, dtype=self.dt.np)
+        assert x.size >= self.ncols * k
+        y = np.zeros((self.nrows, k) if k > 1 else self.nrows, dtype=self.dt.np)
         check(lib().sparsep_execute_host(self.h, x.ctypes.data, y.ctypes.data), "execute_host")
         return y
 

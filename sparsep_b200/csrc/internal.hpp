@@ -125,4 +125,11 @@ void greedy_split_bcsr(const uint64_t *prefix, uint32_t n, uint32_t parts, uint3
 // Text of the last failure, returned by sparsep_last_error() on this thread.
 void record_error(const char *msg);
 
+// sparsep_opts.autotune on a CSR input (autotune.cu): the plan of the variant
+// chosen by timing (2) or by the learned selector (1).
+template <typename T>
+int plan_autotuned(const typename Types<T>::csr *A, const sparsep_opts &o, sparsep_plan **out);
+// Records in the plan's info.variant which variant autotuning chose and how.
+void note_variant(sparsep_plan *p, const char *name, int mode);
+
 }  // namespace sparsep

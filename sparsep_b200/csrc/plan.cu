@@ -93,9 +93,19 @@ struct sparsep_plan {
     void *part = nullptr;
     uint64_t n_vptr = 0, n_h = 0, n_lptr = 0, n_l = 0, n_part = 0;
   } split;
+  // nrhs > 1 (1D CSR, FP32 / INT32): the plan wraps a one-matrix batch, whose
+  // row routines read each nonzero's k right-hand sides together
+  sparsep_batch *batch = nullptr;
 };
 
 static thread_local char g_last_error[256] = "";
+
+namespace sparsep {
+void note_variant(sparsep_plan *p, const char *name, int mode) {
+  if (!p || !name) return;
+  std::snprintf(p->info.variant, sizeof p->info.variant, "%s (%s)", name, mode == 1 ? "learned" : "autotuned");
+}
+}  // namespace sparsep
 
 namespace sparsep {
 void record_error(const char *msg) { std::snprintf(g_last_error, sizeof g_last_error, "%s", msg); }
@@ -178,7 +188,8 @@ static int check_opts(const sparsep_opts *o) {
   if (o->worker_balance < 0 || o->worker_balance > SPARSEP_BAL_INTERLEAVE) return SPARSEP_EINVAL;
   if (o->sync < 0 || o->sync > SPARSEP_SYNC_CG) return SPARSEP_EINVAL;
   if (o->autotune < 0 || o->autotune > 2 || o->heavy_rows < -1) return SPARSEP_EINVAL;
-  if (o->nrhs > 1) return SPARSEP_ENOSYS;
+  if (o->nrhs < 0) return SPARSEP_EINVAL;
+  if (o->nrhs > 256) return SPARSEP_ENOSYS;
   return SPARSEP_OK;
 }
 
@@ -473,6 +484,11 @@ static int begin_plan(sparsep_plan **out, int dtype, int format, int scheme, con
   if (st) return st;
   if (o) oo = *o;
   else sparsep_opts_default(&oo);
+  if (oo.autotune) return SPARSEP_ENOSYS;  // plan variants start from a host CSR (plan_csr)
+  // several right-hand sides: 1D CSR in FP32 / INT32 with automatic items
+  if (oo.nrhs > 1 && !(format == SPARSEP_FMT_CSR && scheme == SPARSEP_1D &&
+                       (dtype == SPARSEP_FP32 || dtype == SPARSEP_INT32) && oo.nr_parts == 0))
+    return SPARSEP_ENOSYS;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   auto *p = new (std::nothrow) sparsep_plan();
@@ -763,11 +779,56 @@ static int build_split(sparsep_plan *p, const typename Types<T>::csr *A, uint32_
 }
 
 // ---------------------------------------------------------------------------
+// Several right-hand sides on one plan: x is ncols x k and y nrows x k, both
+// row-major (one nonzero's k right-hand sides contiguous).  The plan wraps a
+// batch of this one matrix, whose work items read the k values of x a nonzero
+// needs with one load per lane group (the batch's row routines, default
+// variant for k).
+// ---------------------------------------------------------------------------
+template <typename T>
+static int plan_multi_rhs(sparsep_plan *p, const typename Types<T>::csr *A, uint32_t k) {
+  const typename Types<T>::csr *mats[1] = {A};
+  int st;
+  if constexpr (std::is_same<T, float>::value) st = sparsep_batch_create_f32(1, mats, &k, nullptr, &p->batch);
+  else st = sparsep_batch_create_i32(1, mats, &k, nullptr, &p->batch);
+  if (st) return st;
+  if ((st = sparsep_batch_x(p->batch, 0, &p->xpad, &p->y))) return st;  // the batch owns them
+  uint64_t cb = 0, items = 0, nnz = 0;
+  sparsep_batch_get_info(p->batch, &cb, &items, &nnz);
+  p->nrhs = (int)k;
+  p->info.dtype = p->dtype;
+  p->info.format = SPARSEP_FMT_CSR;
+  p->info.scheme = SPARSEP_1D;
+  p->info.nrhs = (int32_t)k;
+  p->info.nrows = p->nrows;
+  p->info.ncols = p->ncols;
+  p->info.nnz = p->nnz;
+  p->info.items = items;
+  p->info.compulsory_bytes = cb;
+  p->info.kernel_launches = 1;
+  sparsep_batch_variant v{};
+  sparsep_batch_get_variant(p->batch, 0, &v);
+  std::snprintf(p->info.variant, sizeof p->info.variant, "csr/1d/rows x %u rhs/%s/lanes=%d/vec=%d", k,
+                v.mode ? "merge" : "rows", v.lanes, v.vec);
+  for (auto &e : p->ev) CK(cudaEventCreate(&e));
+  return SPARSEP_OK;
+}
+
+// ---------------------------------------------------------------------------
 // CSR
 // ---------------------------------------------------------------------------
 template <typename T>
 static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, sparsep_plan **out,
                     bool device_arrays = false) {
+  if (o && o->autotune) {  // one of the plan variants, timed or learned (autotune.cu)
+    if (!out) return SPARSEP_EINVAL;
+    *out = nullptr;
+    if (int st = check_opts(o)) return st;
+    if (device_arrays || o->nrhs > 1) return SPARSEP_ENOSYS;
+    if (!A || (A->nrows && !A->rowptr) || (A->nnz && (!A->colind || !A->values))) return SPARSEP_EINVAL;
+    if (A->rowptr[0] != 0 || A->rowptr[A->nrows] != A->nnz) return SPARSEP_EINVAL;
+    return plan_autotuned<T>(A, *o, out);
+  }
   sparsep_plan *p = nullptr;
   sparsep_opts oo;
   int st = begin_plan(out, Types<T>::dtype, SPARSEP_FMT_CSR, SPARSEP_1D, o, &p, oo);
@@ -784,6 +845,16 @@ static int plan_csr(const typename Types<T>::csr *A, const sparsep_opts *o, spar
   p->nrows = A->nrows;
   p->ncols = A->ncols;
   p->nnz = A->nnz;
+  if (oo.nrhs > 1) {
+    if (device_arrays) return SPARSEP_ENOSYS;  // the batch reads the host arrays
+    if constexpr (std::is_same<T, float>::value || std::is_same<T, int32_t>::value) {
+      if ((st = plan_multi_rhs<T>(p, A, (uint32_t)oo.nrhs))) return st;
+      p->t[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      *out = guard.release();
+      return SPARSEP_OK;
+    }
+    return SPARSEP_ENOSYS;
+  }
   std::vector<Item> items;
   Tile t;
   t.row_end = A->nrows;
@@ -1651,8 +1722,26 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s, un
   return SPARSEP_OK;
 }
 
+// A multi-RHS plan on device buffers: x into the batch, one launch, y out
+// (stream-ordered on s; on the legacy stream, synchronous around the batch's
+// own stream).
+static int run_multi(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
+  const size_t xb = (size_t)p->ncols * p->nrhs * p->esize, yb = (size_t)p->nrows * p->nrhs * p->esize;
+  if (!s) {
+    if (d_x != p->xpad) CK(cudaMemcpy(p->xpad, d_x, xb, cudaMemcpyDeviceToDevice));
+    if (int st = sparsep_batch_execute(p->batch, nullptr)) return st;
+    if (d_y != p->y) CK(cudaMemcpy(d_y, p->y, yb, cudaMemcpyDeviceToDevice));
+    return SPARSEP_OK;
+  }
+  if (d_x != p->xpad) CK(cudaMemcpyAsync(p->xpad, d_x, xb, cudaMemcpyDeviceToDevice, s));
+  if (int st = sparsep_batch_execute(p->batch, s)) return st;
+  if (d_y != p->y) CK(cudaMemcpyAsync(d_y, p->y, yb, cudaMemcpyDeviceToDevice, s));
+  return SPARSEP_OK;
+}
+
 static int run_any(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s,
                    unsigned int *band_cnt = nullptr) {
+  if (p->batch) return run_multi(p, d_x, d_y, s);
   switch (p->dtype) {
     case SPARSEP_INT8: return run_t<int8_t>(p, d_x, d_y, s, band_cnt);
     case SPARSEP_INT16: return run_t<int16_t>(p, d_x, d_y, s, band_cnt);
@@ -1817,6 +1906,7 @@ int sparsep_device_sms(void) {
 
 void sparsep_plan_free(sparsep_plan *p) {
   if (!p) return;
+  if (p->batch) sparsep_batch_free(p->batch);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->copy_stream) {
     cudaStreamSynchronize(p->copy_stream);
@@ -1879,6 +1969,21 @@ static int copy_y_banded(sparsep_plan *p, void *h_y) {
 
 int sparsep_execute_host(sparsep_plan *p, const void *h_x, void *h_y) {
   if (!p || !h_x || !h_y) return SPARSEP_EINVAL;
+  if (p->batch) {  // several right-hand sides: the batch's host copies around one launch
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    int st = sparsep_batch_set_x(p->batch, 0, h_x);
+    const auto t1 = clk::now();
+    if (!st) st = sparsep_batch_execute(p->batch, nullptr);
+    const auto t2 = clk::now();
+    if (!st) st = sparsep_batch_get_y(p->batch, 0, h_y);
+    const auto t3 = clk::now();
+    p->t[1] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    p->t[2] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    p->t[3] = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    p->t[4] = 0;
+    return st;
+  }
   cudaStream_t s = p->stream;
   CK(cudaEventRecord(p->ev[0], s));
   CK(cudaMemcpyAsync(p->xpad, h_x, (size_t)p->ncols * p->esize, cudaMemcpyHostToDevice, s));

@@ -2,9 +2,10 @@
  * converter and free names (readCOOMatrix, coo2csr, csr2bcsr, bcsr2bcoo,
  * free*Matrix) and val_dt from sparsep_compat.h with -DSPARSEP_REFERENCE_NAMES
  * and -D<TYPE>, then the SpMV through the C-ABI in CSR (one-shot, 64 parts by
- * nonzeros, and a plan run twice on host buffers), BCSR 4x4 and BCOO 4x4.
+ * nonzeros, and a plan run twice on host buffers), BCSR 4x4, BCOO 4x4 and the
+ * plan variant the learned selector picks (autotune = 1).
  * Usage: ref_app <file.mtx> <out-prefix>; writes <prefix>.{rowptr,colind,
- * values,x,y_csr,y_plan,y_bcsr,y_bcoo} as raw arrays for the test to check. */
+ * values,x,y_csr,y_plan,y_bcsr,y_bcoo,y_auto} as raw arrays for the test to check. */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -30,8 +31,8 @@ int main(int argc, char **argv) {
   struct BCOOMatrix *Bo = Bc ? bcsr2bcoo(Bc) : NULL;
   if (!Bo) return 4;
   val_dt *x = calloc(A->ncols + 16, sizeof(val_dt));
-  val_dt *y[4];
-  for (int k = 0; k < 4; ++k) y[k] = calloc(A->nrows + 8, sizeof(val_dt));
+  val_dt *y[5];
+  for (int k = 0; k < 5; ++k) y[k] = calloc(A->nrows + 8, sizeof(val_dt));
   for (uint32_t i = 0; i < A->ncols; ++i) x[i] = (val_dt)((int)(i % 7) - 3);
   sparsep_opts o;
   sparsep_opts_default(&o);
@@ -46,6 +47,16 @@ int main(int argc, char **argv) {
   sparsep_plan_free(plan);
   if (!st) st = sparsep_spmv_bcsr(Bc, x, y[2], NULL);
   if (!st) st = sparsep_spmv_bcoo(Bo, x, y[3], NULL);
+  /* the plan variant chosen by the learned selector (autotune = 1) */
+  sparsep_opts ao;
+  sparsep_opts_default(&ao);
+  ao.autotune = 1;
+  if (!st) st = sparsep_plan_csr(A, &ao, &plan);
+  if (!st) st = sparsep_execute_host(plan, x, y[4]);
+  sparsep_plan_info info;
+  if (!st) st = sparsep_plan_get_info(plan, &info);
+  if (!st) fprintf(stderr, "autotune=1 chose %s\n", info.variant);
+  sparsep_plan_free(plan);
   if (st) {
     fprintf(stderr, "ref_app: %s %s\n", sparsep_strerror(st), sparsep_last_error());
     return 5;
@@ -57,13 +68,14 @@ int main(int argc, char **argv) {
             dump(p, "y_csr", y[0], (size_t)A->nrows * sizeof(val_dt)) |
             dump(p, "y_plan", y[1], (size_t)A->nrows * sizeof(val_dt)) |
             dump(p, "y_bcsr", y[2], (size_t)A->nrows * sizeof(val_dt)) |
-            dump(p, "y_bcoo", y[3], (size_t)A->nrows * sizeof(val_dt));
+            dump(p, "y_bcoo", y[3], (size_t)A->nrows * sizeof(val_dt)) |
+            dump(p, "y_auto", y[4], (size_t)A->nrows * sizeof(val_dt));
   printf("%u %u %u\n", A->nrows, A->ncols, A->nnz);
   freeBCOOMatrix(Bo);
   freeBCSRMatrix(Bc);
   freeCSRMatrix(A);
   freeCOOMatrix(B);
   free(x);
-  for (int k = 0; k < 4; ++k) free(y[k]);
+  for (int k = 0; k < 5; ++k) free(y[k]);
   return bad ? 6 : 0;
 }

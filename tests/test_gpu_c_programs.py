@@ -3,7 +3,8 @@
 tests/ref_app.c reads a Matrix Market file with the reference's own reader
 name (readCOOMatrix), converts it with coo2csr / csr2bcsr / bcsr2bcoo,
 multiplies through the C-ABI as CSR (one-shot over 64 nnz-balanced parts, and
-a plan run twice on host buffers), BCSR 4x4 and BCOO 4x4, and writes its
+a plan run twice on host buffers), BCSR 4x4, BCOO 4x4 and the plan variant
+the learned selector picks (sparsep_opts.autotune = 1), and writes its
 arrays.  The results must equal the oracle's (the reference's spmv_host
 restated) on the CSR the program built: integers bit for bit, FP32 / FP64
 within the per-row gamma bound of a long-double sum."""
@@ -52,7 +53,7 @@ def test_reference_style_program_runs(tmp_path, dtype):
     rp, ci, vv, x = ld("rowptr", np.uint32), ld("colind", np.uint32), ld("values", T), ld("x", T)
     assert rp.size == n + 1 and ci.size == nnz == rows.size
     A = sp.csr(dtype, n, m, rp, ci, vv)
-    for name in ("y_csr", "y_plan", "y_bcsr", "y_bcoo"):
+    for name in ("y_csr", "y_plan", "y_bcsr", "y_bcoo", "y_auto"):
         y = ld(name, T)
         if dtype in ("f32", "f64"):
             r = np.repeat(np.arange(n, dtype=np.uint32), np.diff(rp.astype(np.int64)))
