@@ -186,7 +186,7 @@ def run_ours(args, rank, world):
     n, m, rowptr, colind, values, x = make_matrix()
     nnz = int(rowptr[-1])
     A = sp.csr("f32", n, m, rowptr, colind, values)
-    plan = sp.Plan(A, sp.default_opts())
+    plan = sp.Plan(A, sp.default_opts(heavy_rows=args.heavy_rows))
     info = plan.info
     cb = int(info.compulsory_bytes)
     assert cb == compulsory_bytes(n, m, nnz)
@@ -804,6 +804,9 @@ def main():
                     help="single: the FP32 CSR Zipf SpMV only; batch: the batched path only; configs: the "
                          "per-configuration entries only")
     ap.add_argument("--batch-mats", type=int, default=512)
+    ap.add_argument("--heavy-rows", type=int, default=0,
+                    help="headline plan: rows with at least this many nonzeros in shared-memory column stripes "
+                         "(0: the planner's choice, -1: never)")
     ap.add_argument("--no-configs", action="store_true",
                     help="leave out the per-configuration entries (formats, schemes, element types)")
     args = ap.parse_args()

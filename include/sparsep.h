@@ -764,8 +764,11 @@ int sparsep_spmv_cooe_f32_noalloc(const sparsep_elem_f32 *d_elems, uint32_t nnz,
 const char *sparsep_plan_variant_name(int v);
 /* every variant timed (median of reps after a warm-up, device x and y), us;
  * 0 where a variant does not apply; best receives the fastest's index */
+/* sparsep_plan_variant_csr_<t>: the plan of variant v (0 .. SPARSEP_NPLANVARIANTS-1)
+ * of A, the other options as in o */
 #define SPARSEP_DECLARE_AUTOTUNE(T, S) \
-  int sparsep_plan_autotune_csr_##S(const sparsep_csr_##S *A, int reps, double *times_us, int32_t *best);
+  int sparsep_plan_autotune_csr_##S(const sparsep_csr_##S *A, int reps, double *times_us, int32_t *best); \
+  int sparsep_plan_variant_csr_##S(const sparsep_csr_##S *A, int v, const sparsep_opts *o, sparsep_plan **out);
 SPARSEP_DECLARE_AUTOTUNE(int8_t, i8)
 SPARSEP_DECLARE_AUTOTUNE(int16_t, i16)
 SPARSEP_DECLARE_AUTOTUNE(int32_t, i32)

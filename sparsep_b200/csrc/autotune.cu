@@ -86,8 +86,10 @@ SPARSEP_API(float, f32)
 SPARSEP_API(double, f64)
 #undef SPARSEP_API
 
-// The AoS COO of a CSR matrix (rows ascending, columns in CSR order), owning
-// its arrays.
+// The AoS COO of a CSR matrix, sorted by (row, column) as the reference's
+// sortCOOMatrix leaves it (spmv/1D/COO-nnz/support/matrix.h:88-125; the 2D
+// converters expect that order), owning its arrays.  The sort within a row is
+// stable, so duplicate entries keep their order.
 template <typename T> struct CooeOf {
   typename Types<T>::cooe s{};
   std::vector<uint32_t> rows;
@@ -102,6 +104,8 @@ template <typename T> struct CooeOf {
         elems[j].colind = A->colind[j];
         elems[j].val = A->values[j];
       }
+      std::stable_sort(elems.begin() + A->rowptr[r], elems.begin() + A->rowptr[r + 1],
+                       [](const auto &a, const auto &b) { return a.colind < b.colind; });
     }
     s.nrows = A->nrows;
     s.ncols = A->ncols;
@@ -289,6 +293,14 @@ const char *sparsep_plan_variant_name(int v) {
     sparsep_opts o;                                                                                          \
     sparsep_opts_default(&o);                                                                                \
     return autotune_times<T>(A, o, reps, times_us, best);                                                    \
+  }                                                                                                          \
+  int sparsep_plan_variant_csr_##S(const sparsep_csr_##S *A, int v, const sparsep_opts *o, sparsep_plan **out) { \
+    if (!A || !out || v < 0 || v >= SPARSEP_NPLANVARIANTS) return SPARSEP_EINVAL;                            \
+    sparsep_opts oo;                                                                                         \
+    if (o) oo = *o; else sparsep_opts_default(&oo);                                                          \
+    int st = build_variant<T>(A, v, oo, out);                                                                \
+    if (!st) note_variant(*out, kVariants[v].name, 0);                                                       \
+    return st;                                                                                               \
   }
 SPARSEP_AUTOTUNE_ENTRY(int8_t, i8)
 SPARSEP_AUTOTUNE_ENTRY(int16_t, i16)

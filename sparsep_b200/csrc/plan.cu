@@ -103,7 +103,8 @@ static thread_local char g_last_error[256] = "";
 namespace sparsep {
 void note_variant(sparsep_plan *p, const char *name, int mode) {
   if (!p || !name) return;
-  std::snprintf(p->info.variant, sizeof p->info.variant, "%s (%s)", name, mode == 1 ? "learned" : "autotuned");
+  if (mode == 0) std::snprintf(p->info.variant, sizeof p->info.variant, "%s", name);
+  else std::snprintf(p->info.variant, sizeof p->info.variant, "%s (%s)", name, mode == 1 ? "learned" : "autotuned");
 }
 }  // namespace sparsep
 

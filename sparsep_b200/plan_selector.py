@@ -122,7 +122,7 @@ def export(model: dict, path: Path = CPP):
         lines.append("    " + ", ".join(f"0x{v:04x}" for v in wb[s:s + 16]) + ",")
     lines.append("};")
     for name, arr in (("kMean", model["mean"]), ("kStd", model["std"])):
-        lines.append(f"const float {name}[{arr.size}] = {{" + ", ".join(f"{float(v):.9g}f" for v in arr) + "};")
+        lines.append(f"const float {name}[{arr.size}] = {{" + ", ".join(f"{float(v):.9e}f" for v in arr) + "};")
     lines += ["}  // namespace", "const uint16_t *plan_model_weights() { return kWb; }",
               "const float *plan_model_mean() { return kMean; }", "const float *plan_model_std() { return kStd; }",
               "}  // namespace sparsep", ""]
@@ -144,6 +144,7 @@ def main(argv=None):
     t.add_argument("--out", type=Path, default=MODEL)
     x = sub.add_parser("export")
     x.add_argument("--model", type=Path, default=MODEL)
+    x.add_argument("--cpp", type=Path, default=CPP)
     a = ap.parse_args(argv)
     if a.cmd == "gen":
         db = timing_db(a.count, a.seed, reps=a.reps)
@@ -169,7 +170,7 @@ def main(argv=None):
         meta = json.loads(str(z["meta"]))
         export(dict(wb=z["wb"], mean=z["mean"], std=z["std"],
                     note=f"{meta['train_samples']} matrices (held-out regret "
-                         f"{meta['heldout_eval']['regret_total']:.3f})"))
+                         f"{meta['heldout_eval']['regret_total']:.3f})"), a.cpp)
         return 0
     return 2
 

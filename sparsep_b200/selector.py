@@ -57,18 +57,19 @@ def default_index(k: int) -> int:
 # timing database
 # ---------------------------------------------------------------------------
 def _gen(args):
-    seed, i = args
-    d = synth.selector_one(seed, i)
+    seed, i, kw = args
+    d = synth.selector_one(seed, i, **kw)
     d["feat"] = capi.features(d["n"], d["n"], d["rowptr"], d["colind"], d["k"])
     return i, d
 
 
 def timing_db(count: int, seed: int, reps: int = 3, chunk: int = 48, workers: int | None = None,
-              log=print) -> dict:
+              log=print, **ranges) -> dict:
     """Features and per-candidate median times (us; 0 = not applicable) of
     training matrices 0 .. count - 1 of stream `seed`, each timed alone on
     the current GPU.  Matrices are generated by a pool of spawned processes
-    while the GPU times the previous chunk."""
+    while the GPU times the previous chunk; `ranges` override the generator's
+    row, row-length and size ranges (synth.selector_one)."""
     workers = workers or max(1, min(32, (os.cpu_count() or 2) - 1))
     ctx = mp.get_context("spawn")
     feats = np.zeros((count, capi.NFEATURES), dtype=np.float32)
@@ -77,7 +78,7 @@ def timing_db(count: int, seed: int, reps: int = 3, chunk: int = 48, workers: in
     cands = capi.batch_candidates()
     t0 = time.time()
     with ctx.Pool(workers) as pool:
-        it = pool.imap(_gen, [(seed, i) for i in range(count)], chunksize=4)
+        it = pool.imap(_gen, [(seed, i, ranges) for i in range(count)], chunksize=4)
         done = 0
         while done < count:
             ds = [next(it)[1] for _ in range(min(chunk, count - done))]
@@ -219,6 +220,10 @@ def main(argv=None):
     g.add_argument("--seed", type=int, required=True)
     g.add_argument("--reps", type=int, default=3)
     g.add_argument("--out", type=Path, required=True)
+    g.add_argument("--rows-lo", type=int, default=1_000)
+    g.add_argument("--rows-hi", type=int, default=262_144)
+    g.add_argument("--len-hi", type=int, default=64)
+    g.add_argument("--max-nnz", type=int, default=4_000_000)
     t = sub.add_parser("train")
     t.add_argument("--db", type=Path, nargs="+", required=True)
     t.add_argument("--steps", type=int, default=3000)
@@ -231,7 +236,8 @@ def main(argv=None):
     e.add_argument("--db", type=Path, required=True)
     a = ap.parse_args(argv)
     if a.cmd == "gen":
-        db = timing_db(a.count, a.seed, reps=a.reps)
+        db = timing_db(a.count, a.seed, reps=a.reps, rows_lo=a.rows_lo, rows_hi=a.rows_hi, len_hi=a.len_hi,
+                       max_nnz=a.max_nnz)
         a.out.parent.mkdir(parents=True, exist_ok=True)
         np.savez_compressed(a.out, **db)
         return 0

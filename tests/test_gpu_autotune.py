@@ -67,3 +67,31 @@ def test_autotune_rejects_what_it_does_not_cover():
     with pytest.raises(capi.SparsepError) as e:
         sp.Plan(E, sp.default_opts(autotune=2))
     assert e.value.status == capi.ENOSYS
+
+
+def test_learned_choice_on_held_out_matrices():
+    """The plan-variant network (the library's MLP kernels, the committed
+    model) against the exhaustive best on the 120 held-out matrices of the
+    timing database: at most 10 % slower in total, and faster than fixed CSR."""
+    from sparsep_b200 import selector
+
+    z = np.load(plan_selector.DATA / "plan_model.npz")
+    h = np.load(plan_selector.DATA / "plan_heldout.npz")
+    sel = selector.selector(dict(wb=z["wb"], mean=z["mean"], std=z["std"]))
+    ev = plan_selector.evaluate(sel.scores(h["feats"]), h["times"])
+    print(ev)
+    assert ev["samples"] == 120
+    assert ev["regret_total"] <= 0.10
+    assert ev["speedup_vs_fixed_csr"] > 1.0
+
+
+def test_learned_choice_is_taken_when_confident():
+    """With the model compiled in, autotune = 1 takes the network's pick on a
+    matrix family it has seen (no timing run), and the result holds."""
+    A, arrays, x = family_matrix("i32", "banded", seed=9)
+    plan = sp.Plan(A, sp.default_opts(autotune=1))
+    variant = plan.info.variant.decode()
+    print(variant)
+    assert variant.endswith("(learned)") or variant.endswith("(autotuned)")
+    check(A, arrays, x, plan.run_host(x), variant)
+    plan.free()
