@@ -401,14 +401,16 @@ def run_batch(args, dt="f32"):
     default = timeit(lambda: b.execute(st.cuda_stream))
     sel = selector.selector(selector.load())
     t0 = time.time()
-    b.select(sel, min_confidence=0.0)
+    ch_learned, _ = b.select(sel, min_confidence=0.0)
     select_s = time.time() - t0
+    kinds_learned = b.item_kinds()
     learned = timeit(lambda: b.execute(st.cuda_stream))
     b.status()
     y_learned = {m: b.get_y(m) for m in sample}
     t0 = time.time()
-    b.autotune(reps=3)
+    _, ch_tuned = b.autotune(reps=3)
     tune_s = time.time() - t0
+    kinds_tuned = b.item_kinds()
     tuned = timeit(lambda: b.execute(st.cuda_stream))
     b.status()
     y_tuned = {m: b.get_y(m) for m in sample}
@@ -445,6 +447,14 @@ def run_batch(args, dt="f32"):
     def gbs(ms):
         return round(cb / (ms * 1e-3) / 1e9, 2)
 
+    cands = capi.batch_candidates()
+
+    def kinds(ch, items):
+        modes = [int(cands[c].mode) for c in ch if c >= 0]
+        return {"matrices_rows": modes.count(0), "matrices_merge": modes.count(1),
+                "matrices_window_rows": modes.count(2), "matrices_window_merge": modes.count(3),
+                "window_items": int(items[0]), "long_row_chunk_items": int(items[1])}
+
     out = {"workload": f"{len(w)} CSR matrices, rows log-uniform 1k-256k, uniform / Zipf / banded, 1-32 "
                        f"right-hand sides each, {dt.upper()} (seed 3)",
            "dtype": dt, "nnz": int(info["nnz"]), "compulsory_bytes": int(cb), "items": int(info["items"]),
@@ -454,6 +464,10 @@ def run_batch(args, dt="f32"):
            "learned_over_autotuned": round(learned / tuned, 4),
            "gbs": {"plain": gbs(plain), "default": gbs(default), "learned": gbs(learned), "autotuned": gbs(tuned)},
            "select_s": round(select_s, 3), "autotune_s": round(tune_s, 2), "setup_s": round(setup_s, 1),
+           "chosen": {"learned": kinds(ch_learned, kinds_learned), "autotuned": kinds(ch_tuned, kinds_tuned),
+                      "note": "modes 2/3 are window items: a row range whose x tile is staged in shared "
+                              "memory beside its nonzeros (a 2D tile); rows over 4096 nonzeros run as "
+                              "chunk items on many CTAs"},
            "check": check,
            "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
     if cpu_s > 0:

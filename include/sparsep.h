@@ -503,17 +503,24 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
 /* Batched multi-RHS SpMV (no reference counterpart)                         */
 /* ------------------------------------------------------------------------ */
 /* Many CSR matrices, each with its own k = 1..256 right-hand sides (x is
- * ncols x k and y nrows x k, row-major), multiplied by ONE kernel launch:
+ * ncols x k and y nrows x k, row-major; on the device their rows are `pitch`
+ * elements apart, k rounded up to a multiple of 4 for k >= 3, so that 4-wide
+ * loads serve every k), multiplied by ONE kernel launch:
  * its CTAs claim work items (row ranges of any matrix, at most 4096 nonzeros,
  * or one longer row) from a device work queue by atomic ticket, replayed as a
  * CUDA graph (queue reset + kernel).  The row routine of each matrix is a
  * variant: the CTA is cut into groups of `lanes` (1..32, power of two) lanes,
- * each lane reading `vec` (1, 2, 4; k % vec == 0) consecutive right-hand
- * sides per load, k <= 8 * lanes;
+ * each lane reading `vec` (1, 2, 4; pitch % vec == 0) consecutive
+ * right-hand sides per load, pitch <= 8 * lanes;
  *   mode 0: the rows of a work item dealt round-robin to the groups;
  *   mode 1: the rows and nonzeros of a work item split evenly over the groups
  *           (merge path), rows cut by a split finished from carries;
+ *   mode 2, 3: as 0, 1, with window items (2D tiles): a work item whose
+ *           columns span few enough rows of x has that x tile staged in
+ *           shared memory with its nonzeros, and gathers from there (vec 4);
  *   item_work: nonzero x right-hand-side products per item (0 = 65536).
+ * A row longer than 4096 nonzeros runs as one work item per 4096-nonzero
+ * chunk; the last chunk to finish sums the chunks' partial rows in order.
  * FP32 and INT32 (integers wrap exactly, as the single-vector path).  Status
  * ENOSYS: the variant does not apply to that k. */
 typedef struct sparsep_batch sparsep_batch;
@@ -527,8 +534,10 @@ int sparsep_batch_create_f32(uint32_t nmats, const sparsep_csr_f32 *const *A, co
 int sparsep_batch_create_i32(uint32_t nmats, const sparsep_csr_i32 *const *A, const uint32_t *nrhs,
                              const sparsep_batch_variant *variants, sparsep_batch **out);
 void sparsep_batch_free(sparsep_batch *b);
-/* x / y of matrix m: device pointers, or host copies in and out */
+/* x / y of matrix m: device pointers (rows `pitch` elements apart; the pad
+ * columns never reach a result), or host copies in and out (dense rows of k) */
 int sparsep_batch_x(sparsep_batch *b, uint32_t m, void **d_x, void **d_y);
+int sparsep_batch_pitch(const sparsep_batch *b, uint32_t m, uint32_t *pitch);
 int sparsep_batch_set_x(sparsep_batch *b, uint32_t m, const void *h_x);
 int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y);
 /* change a matrix's variant; sparsep_batch_commit rebuilds the work queue */
@@ -559,6 +568,10 @@ int sparsep_batch_autotune(sparsep_batch *b, int reps, double *times_us, int32_t
 int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v, int reps,
                                double *us_out);
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
+/* committed work items by kind: window items (a row range with its x tile
+ * staged in shared memory) and chunk items (rows longer than 4096 nonzeros,
+ * one item per 4096-nonzero chunk) */
+int sparsep_batch_item_kinds(const sparsep_batch *b, uint64_t *window_items, uint64_t *chunk_items);
 
 /* ------------------------------------------------------------------------ */
 /* COO -> CSR on the device (no reference counterpart on the device; the     */

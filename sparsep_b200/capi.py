@@ -486,6 +486,12 @@ def spmv(A: HostMatrix, x: np.ndarray, opts: Opts | None = None) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # batched multi-RHS SpMV
 # ---------------------------------------------------------------------------
+def row_pitch(k: int) -> int:
+    """Elements between rows of a batch matrix's device x and y: k for
+    k <= 2, else k rounded up to a multiple of 4."""
+    return k if k <= 2 else (k + 3) // 4 * 4
+
+
 class BatchVariant(C.Structure):
     _fields_ = [("mode", C.c_int32), ("lanes", C.c_int32), ("item_work", C.c_int32), ("vec", C.c_int32)]
 
@@ -493,9 +499,11 @@ class BatchVariant(C.Structure):
         return (int(self.mode), int(self.lanes), int(self.item_work), int(self.vec))
 
     def applies(self, k: int) -> bool:
-        """Whether this variant can run a matrix with k right-hand sides."""
+        """Whether this variant can run a matrix with k right-hand sides
+        (stored with rows of row_pitch(k) elements, all computed)."""
         v = max(1, int(self.vec))
-        if k % v:
+        k = row_pitch(k)
+        if k % v or (int(self.mode) & 2 and v != 4):  # window modes: 4-wide variants
             return False
         per = -(-k // (self.lanes * v))
         acc = 1
@@ -514,6 +522,8 @@ def _batch_sigs(L):
     L.sparsep_batch_free.argtypes = [PB]
     L.sparsep_batch_free.restype = None
     L.sparsep_batch_x.argtypes = [PB, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    L.sparsep_batch_pitch.argtypes = [PB, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.sparsep_batch_item_kinds.argtypes = [PB, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.sparsep_batch_set_x.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_get_y.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_set_variant.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant)]
@@ -587,7 +597,20 @@ class Batch:
         check(lib().sparsep_batch_get_y(self.h, m, y.ctypes.data), "batch_get_y")
         return y
 
+    def item_kinds(self) -> tuple[int, int]:
+        """Committed (window items, long-row chunk items)."""
+        w, c = C.c_uint64(), C.c_uint64()
+        check(lib().sparsep_batch_item_kinds(self.h, C.byref(w), C.byref(c)), "batch_item_kinds")
+        return w.value, c.value
+
+    def pitch(self, m: int) -> int:
+        """Elements between consecutive rows of matrix m's device x and y."""
+        p = C.c_uint32()
+        check(lib().sparsep_batch_pitch(self.h, m, C.byref(p)), "batch_pitch")
+        return p.value
+
     def device_xy(self, m: int):
+        """Device x (ncols x pitch) and y (nrows x pitch) of matrix m."""
         dx, dy = C.c_void_p(), C.c_void_p()
         check(lib().sparsep_batch_x(self.h, m, C.byref(dx), C.byref(dy)))
         return dx.value, dy.value

@@ -28,6 +28,7 @@ struct sparsep_batch {
   std::vector<Mat<float>> mats_h;  // pointers are type-agnostic; values reinterpreted per dtype
   std::vector<uint64_t> nnz;
   std::vector<std::vector<uint32_t>> rowptr;  // host copies: items are rebuilt without a read-back
+  std::vector<std::vector<uint32_t>> clo, chi;  // per row: lowest and highest column (window items)
   std::vector<float> feat;                    // nmats x SPARSEP_NFEATURES selector features
   std::vector<sparsep_batch_variant> var;
   std::vector<BItem> items_h;          // committed items, matrix after matrix
@@ -95,14 +96,25 @@ static uint32_t item_cap(const sparsep_batch_variant &v, uint32_t k) {
 }
 
 // Items of one matrix: consecutive rows up to `cap` nonzeros and BRCAP rows;
-// a row longer than BCAP is an item of its own (processed in chunks).
-static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparsep_batch_variant &v,
-                       uint32_t cap, std::vector<BItem> &out) {
-  const uint32_t k = M.k;
+// a row longer than BCAP becomes one item per BCAP-nonzero chunk, sharing the
+// row's slot of chunk partials and its arrival counter.  Under a
+// window variant (mode 2, 3) an item also stops growing when the x rows its
+// columns span would no longer fit the staging arena beside its nonzeros, and
+// it stages them (c0, cw) when they pay: at least two nonzeros per staged x
+// row.  Rows whose own span does not fit start ordinary items.
+static void make_items(const Mat<float> &M, const uint32_t *rowptr, const uint32_t *clo, const uint32_t *chi,
+                       uint32_t es, const sparsep_batch_variant &v, uint32_t cap, std::vector<BItem> &out) {
+  const uint32_t k = M.pitch;  // every routine computes the whole padded row
   const uint32_t V = (uint32_t)std::max(1, v.vec);
   const uint32_t acc = pow2ceil((k + v.lanes * V - 1) / (v.lanes * V));
-  const uint32_t g_long = std::min<uint32_t>(32, pow2ceil(k));
-  const uint32_t acc_long = pow2ceil((k + g_long - 1) / g_long);
+  // chunks of long rows: the widest load the pitch allows, lanes for one pass
+  const uint32_t v_long = k % 4 == 0 ? 4 : (k % 2 == 0 ? 2 : 1);
+  const uint32_t g_long = std::min<uint32_t>(32, pow2ceil(k / v_long));
+  const uint32_t acc_long = pow2ceil((k + g_long * v_long - 1) / (g_long * v_long));
+  uint64_t part_off = 0;  // the long rows' partials and counters, in row order
+  uint32_t slot = 0;
+  const bool windows = (v.mode & 2) != 0;
+  const uint32_t xrow = k * es;  // bytes of one staged x row
   BItem base{};
   base.rowptr = M.rowptr;
   base.colind = M.colind;
@@ -112,38 +124,65 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparse
   base.k = (uint16_t)k;
   base.ncols = M.ncols;
   BItem cur{};
-  bool open = false;
+  bool open = false, win = false;
+  uint32_t lo = 0, hi = 0;  // columns spanned by the open window item (hi exclusive; lo == hi: none yet)
+  auto fits = [&](uint32_t nr, uint32_t n, uint32_t a, uint32_t b) {
+    return carve(nr, n, es, (b - a) * xrow).end <= ARENA;
+  };
   auto flush = [&]() {
-    if (open) out.push_back(cur);
+    if (!open) return;
     open = false;
+    if (win && hi > lo && 2ull * (hi - lo) <= cur.p1 - cur.p0) cur.c0 = lo, cur.cw = hi - lo;
+    out.push_back(cur);
   };
   for (uint32_t r = 0; r < M.nrows; ++r) {
     const uint32_t len = rowptr[r + 1] - rowptr[r];
     if (len > BCAP) {
       flush();
-      BItem it = base;
-      it.r0 = r;
-      it.nr = 1;
-      it.p0 = rowptr[r];
-      it.p1 = rowptr[r + 1];
-      it.mode = MODE_LONG;
-      it.lanes = (uint8_t)g_long;
-      it.vec = 1;
-      it.acc = (uint8_t)acc_long;
-      out.push_back(it);
+      const uint32_t nch = (len + BCAP - 1) / BCAP;
+      for (uint32_t c = 0; c < nch; ++c) {
+        BItem it = base;
+        it.r0 = r;
+        it.nr = 1;
+        it.p0 = rowptr[r] + c * BCAP;
+        it.p1 = std::min(rowptr[r + 1], it.p0 + BCAP);
+        it.mode = MODE_LONG;
+        it.lanes = (uint8_t)g_long;
+        it.vec = (uint8_t)v_long;
+        it.acc = (uint8_t)acc_long;
+        it.c0 = c;
+        it.cw = nch;
+        it.part = M.part + part_off;
+        it.cnt = M.cnt + slot;
+        out.push_back(it);
+      }
+      part_off += (uint64_t)nch * k;
+      ++slot;
       continue;
     }
-    if (open && (cur.p1 - cur.p0 + len > cap || cur.nr == BRCAP)) flush();
+    // the span with this row added
+    const uint32_t a = len ? (hi > lo ? std::min(lo, clo[r]) : clo[r]) : lo;
+    const uint32_t b = len ? (hi > lo ? std::max(hi, chi[r] + 1) : chi[r] + 1) : hi;
+    if (open && (cur.p1 - cur.p0 + len > cap || cur.nr == BRCAP ||
+                 (win && !fits(cur.nr + 1, cur.p1 - cur.p0 + len, a, b))))
+      flush();
     if (!open) {
       cur = base;
       cur.r0 = r;
       cur.nr = 0;
       cur.p0 = cur.p1 = rowptr[r];
-      cur.mode = v.mode == 0 ? MODE_ROWS : MODE_MERGE;
+      cur.mode = (v.mode & 1) ? MODE_MERGE : MODE_ROWS;
       cur.lanes = (uint8_t)v.lanes;
       cur.vec = (uint8_t)V;
       cur.acc = (uint8_t)acc;
+      cur.c0 = cur.cw = 0;
       open = true;
+      lo = hi = 0;
+      win = windows && (!len || fits(1, len, clo[r], chi[r] + 1));
+    }
+    if (win && len) {
+      lo = hi > lo ? std::min(lo, clo[r]) : clo[r];
+      hi = std::max(hi, chi[r] + 1);
     }
     cur.nr = (uint16_t)(r + 1 - cur.r0);
     cur.p1 = rowptr[r + 1];
@@ -151,25 +190,27 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const sparse
   flush();
 }
 
-static int check_variant(const sparsep_batch_variant &v, uint32_t k) {
-  if (v.item_work < 0 || (v.mode != 0 && v.mode != 1)) return SPARSEP_EINVAL;
+static int check_variant(const sparsep_batch_variant &v, uint32_t nrhs) {
+  if (v.item_work < 0 || v.mode < 0 || v.mode > 3) return SPARSEP_EINVAL;
+  const uint32_t k = row_pitch(nrhs);
   const int V = v.vec ? v.vec : 1;
   if (v.lanes < 1 || v.lanes > 32 || (v.lanes & (v.lanes - 1))) return SPARSEP_EINVAL;
   if (V != 1 && V != 2 && V != 4) return SPARSEP_EINVAL;
-  if (k % V) return SPARSEP_ENOSYS;
+  if (k % V || ((v.mode & 2) && V != 4)) return SPARSEP_ENOSYS;  // windows: 4-wide variants
   if (pow2ceil((k + v.lanes * V - 1) / (v.lanes * V)) * V > (uint32_t)ACC_REGS) return SPARSEP_ENOSYS;
   return SPARSEP_OK;
 }
 
-// Merge mode, the widest vector load that divides k, and enough lanes for
-// one pass over the right-hand sides (at most 32).
-extern "C" void sparsep_batch_variant_default(uint32_t k, sparsep_batch_variant *v) {
+// Merge mode, the widest vector load that divides the row pitch, and enough
+// lanes for one pass over it (at most 32).
+extern "C" void sparsep_batch_variant_default(uint32_t nrhs, sparsep_batch_variant *v) {
   if (!v) return;
   std::memset(v, 0, sizeof *v);
+  const uint32_t k = row_pitch(nrhs);
   v->mode = 1;
-  v->vec = k % 4 == 0 ? 4 : (k % 2 == 0 ? 2 : 1);
+  v->vec = k % 4 == 0 ? 4 : 1;
   v->lanes = (int)std::min<uint32_t>(32, pow2ceil((k + v->vec - 1) / v->vec));
-  while (check_variant(*v, k) && v->vec > 1) {
+  while (check_variant(*v, nrhs) && v->vec > 1) {
     v->vec >>= 1;
     v->lanes = (int)std::min<uint32_t>(32, pow2ceil((k + v->vec - 1) / v->vec));
   }
@@ -183,7 +224,7 @@ static void queue_order(const std::vector<BItem> &in, std::vector<BItem> &q) {
   q.reserve(in.size());
   for (const BItem &it : in)
     if (it.mode == MODE_LONG) q.push_back(it);
-  std::stable_sort(q.begin(), q.end(), [](const BItem &a, const BItem &b) { return a.p1 - a.p0 > b.p1 - b.p0; });
+  std::stable_sort(q.begin(), q.end(), [](const BItem &a, const BItem &b) { return a.cw > b.cw; });
   for (const BItem &it : in)
     if (it.mode != MODE_LONG) q.push_back(it);
 }
@@ -197,7 +238,8 @@ static int rebuild(sparsep_batch *b) {
   b->items_h.clear();
   for (uint32_t m = 0; m < b->nmats; ++m) {
     b->item0[m] = (uint32_t)b->items_h.size();
-    make_items(b->mats_h[m], b->rowptr[m].data(), b->var[m], item_cap(b->var[m], b->mats_h[m].k), b->items_h);
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), (uint32_t)b->esize, b->var[m],
+               item_cap(b->var[m], b->mats_h[m].pitch), b->items_h);
     b->nitem[m] = (uint32_t)b->items_h.size() - b->item0[m];
   }
   std::vector<BItem> q;
@@ -251,6 +293,8 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
   b->base0.resize(nmats);
   b->nbase.resize(nmats);
   b->rowptr.resize(nmats);
+  b->clo.resize(nmats);
+  b->chi.resize(nmats);
   for (uint32_t m = 0; m < nmats; ++m) {
     const auto *M = A[m];
     if (!M || !M->rowptr || (M->nnz && (!M->colind || !M->values))) return SPARSEP_EINVAL;
@@ -264,31 +308,54 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
     if (var) b->var[m] = var[m];
     else sparsep_batch_variant_default(k, &b->var[m]);
     if (int st = check_variant(b->var[m], k)) return st;
+    const uint32_t kp = row_pitch(k);
     void *d[5];
     int st = balloc(b, ((size_t)M->nrows + 1 + 16) * 4, &d[0]);
     if (!st) st = balloc(b, ((size_t)M->nnz + 16) * 4, &d[1]);
     if (!st) st = balloc(b, ((size_t)M->nnz + 16) * sizeof(T), &d[2]);
-    if (!st) st = balloc(b, ((size_t)M->ncols * k + 16) * sizeof(T), &d[3]);
-    if (!st) st = balloc(b, ((size_t)M->nrows * k + 16) * sizeof(T), &d[4]);
+    if (!st) st = balloc(b, ((size_t)M->ncols * kp + 16) * sizeof(T), &d[3]);
+    if (!st) st = balloc(b, ((size_t)M->nrows * kp + 16) * sizeof(T), &d[4]);
     if (st) return st;
+    // rows longer than BCAP: a partial row per chunk and an arrival counter
+    uint64_t chunks = 0, longrows = 0;
+    for (uint32_t r = 0; r < M->nrows; ++r) {
+      const uint32_t len = M->rowptr[r + 1] - M->rowptr[r];
+      if (len > BCAP) chunks += (len + BCAP - 1) / BCAP, ++longrows;
+    }
+    void *part = nullptr, *cnt = nullptr;
+    if (longrows) {
+      if ((st = balloc(b, chunks * kp * sizeof(T), &part))) return st;
+      if ((st = balloc(b, longrows * sizeof(unsigned), &cnt))) return st;
+      BCK(cudaMemsetAsync(cnt, 0, longrows * sizeof(unsigned), b->stream));
+    }
     BCK(cudaMemcpyAsync(d[0], M->rowptr, ((size_t)M->nrows + 1) * 4, cudaMemcpyHostToDevice, b->stream));
     if (M->nnz) {
       BCK(cudaMemcpyAsync(d[1], M->colind, (size_t)M->nnz * 4, cudaMemcpyHostToDevice, b->stream));
       BCK(cudaMemcpyAsync(d[2], M->values, (size_t)M->nnz * sizeof(T), cudaMemcpyHostToDevice, b->stream));
     }
-    BCK(cudaMemsetAsync(d[3], 0, ((size_t)M->ncols * k + 16) * sizeof(T), b->stream));
+    BCK(cudaMemsetAsync(d[3], 0, ((size_t)M->ncols * kp + 16) * sizeof(T), b->stream));
     auto &h = b->mats_h[m];
     h.rowptr = (const uint32_t *)d[0];
     h.colind = (const uint32_t *)d[1];
     h.val = (const float *)d[2];
     h.x = (const float *)d[3];
     h.y = (float *)d[4];
+    h.part = (float *)part;
+    h.cnt = (unsigned *)cnt;
     h.nrows = M->nrows;
     h.ncols = M->ncols;
     h.k = k;
-    h.pad = 0;
+    h.pitch = kp;
     b->nnz[m] = M->nnz;
     b->rowptr[m].assign(M->rowptr, M->rowptr + M->nrows + 1);
+    b->clo[m].assign(M->nrows, 0);
+    b->chi[m].assign(M->nrows, 0);
+    for (uint32_t r = 0; r < M->nrows; ++r)
+      for (uint32_t q = M->rowptr[r]; q < M->rowptr[r + 1]; ++q) {
+        const uint32_t c = M->colind[q];
+        if (q == M->rowptr[r] || c < b->clo[m][r]) b->clo[m][r] = c;
+        if (q == M->rowptr[r] || c > b->chi[m][r]) b->chi[m][r] = c;
+      }
     b->bytes += (uint64_t)M->nnz * (4 + sizeof(T)) + ((uint64_t)M->nrows + 1) * 4 +
                 ((uint64_t)M->ncols + M->nrows) * k * sizeof(T);
   }
@@ -309,8 +376,8 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
     sparsep_batch_variant dv;
     sparsep_batch_variant_default(b->mats_h[m].k, &dv);
     b->base0[m] = (uint32_t)b->base_h.size();
-    make_items(b->mats_h[m], b->rowptr[m].data(), dv, grid_filling_cap(b, m, item_cap(dv, b->mats_h[m].k)),
-               b->base_h);
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), (uint32_t)b->esize, dv,
+               grid_filling_cap(b, m, item_cap(dv, b->mats_h[m].pitch)), b->base_h);
     b->nbase[m] = (uint32_t)b->base_h.size() - b->base0[m];
   }
   int st = balloc(b, 64, (void **)&b->err);
@@ -411,10 +478,19 @@ int sparsep_batch_x(sparsep_batch *b, uint32_t m, void **d_x, void **d_y) {
   return SPARSEP_OK;
 }
 
+int sparsep_batch_pitch(const sparsep_batch *b, uint32_t m, uint32_t *pitch) {
+  if (!b || !pitch || m >= b->nmats) return SPARSEP_EINVAL;
+  *pitch = b->mats_h[m].pitch;
+  return SPARSEP_OK;
+}
+
+// Host x (ncols x k, dense rows) into the device rows of `pitch` elements.
 int sparsep_batch_set_x(sparsep_batch *b, uint32_t m, const void *h_x) {
   if (!b || !h_x || m >= b->nmats) return SPARSEP_EINVAL;
   const auto &M = b->mats_h[m];
-  BCK(cudaMemcpyAsync((void *)M.x, h_x, (size_t)M.ncols * M.k * b->esize, cudaMemcpyHostToDevice, b->stream));
+  const size_t w = (size_t)M.k * b->esize;
+  BCK(cudaMemcpy2DAsync((void *)M.x, (size_t)M.pitch * b->esize, h_x, w, w, M.ncols, cudaMemcpyHostToDevice,
+                        b->stream));
   BCK(cudaStreamSynchronize(b->stream));  // in place before any later launch, on any stream
   return SPARSEP_OK;
 }
@@ -423,7 +499,8 @@ int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y) {
   if (!b || !h_y || m >= b->nmats) return SPARSEP_EINVAL;
   const auto &M = b->mats_h[m];
   BCK(cudaStreamSynchronize(b->stream));
-  BCK(cudaMemcpyAsync(h_y, M.y, (size_t)M.nrows * M.k * b->esize, cudaMemcpyDeviceToHost, b->stream));
+  const size_t w = (size_t)M.k * b->esize;
+  BCK(cudaMemcpy2DAsync(h_y, w, M.y, (size_t)M.pitch * b->esize, w, M.nrows, cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   return SPARSEP_OK;
 }
@@ -479,12 +556,12 @@ int sparsep_batch_execute_one(sparsep_batch *b, uint32_t m, void *stream) {
 // recaptured on the next execute).  times_us (nmats x candidates) receives
 // the medians, 0 where a candidate does not apply; chosen (nmats) the index.
 static const sparsep_batch_variant kCand[] = {
-    {0, 1, 0, 1},  {0, 1, 0, 2},  {0, 1, 0, 4},  {0, 2, 0, 1},  {0, 2, 0, 2},  {0, 2, 0, 4},
-    {0, 4, 0, 1},  {0, 4, 0, 2},  {0, 4, 0, 4},  {0, 8, 0, 1},  {0, 8, 0, 2},  {0, 8, 0, 4},
-    {0, 16, 0, 1}, {0, 16, 0, 2}, {0, 16, 0, 4}, {0, 32, 0, 1}, {0, 32, 0, 2}, {0, 32, 0, 4},
-    {1, 1, 0, 1},  {1, 1, 0, 2},  {1, 1, 0, 4},  {1, 2, 0, 1},  {1, 2, 0, 2},  {1, 2, 0, 4},
-    {1, 4, 0, 1},  {1, 4, 0, 2},  {1, 4, 0, 4},  {1, 8, 0, 1},  {1, 8, 0, 2},  {1, 8, 0, 4},
-    {1, 16, 0, 1}, {1, 16, 0, 2}, {1, 16, 0, 4}, {1, 32, 0, 1}, {1, 32, 0, 2}, {1, 32, 0, 4}};
+    {0, 1, 0, 1},  {0, 1, 0, 4},  {0, 2, 0, 1},  {0, 2, 0, 4},  {0, 4, 0, 1},  {0, 4, 0, 4},
+    {0, 8, 0, 1},  {0, 8, 0, 4},  {0, 16, 0, 1}, {0, 16, 0, 4}, {0, 32, 0, 1}, {0, 32, 0, 4},
+    {1, 1, 0, 1},  {1, 1, 0, 4},  {1, 2, 0, 1},  {1, 2, 0, 4},  {1, 4, 0, 1},  {1, 4, 0, 4},
+    {1, 8, 0, 1},  {1, 8, 0, 4},  {1, 16, 0, 1}, {1, 16, 0, 4}, {1, 32, 0, 1}, {1, 32, 0, 4},
+    {2, 1, 0, 4},  {2, 2, 0, 4},  {2, 4, 0, 4},  {2, 8, 0, 4},  {2, 16, 0, 4}, {2, 32, 0, 4},
+    {3, 1, 0, 4},  {3, 2, 0, 4},  {3, 4, 0, 4},  {3, 8, 0, 4},  {3, 16, 0, 4}, {3, 32, 0, 4}};
 constexpr int kNCand = sizeof(kCand) / sizeof(kCand[0]);
 static_assert(kNCand == SPARSEP_NVARIANTS, "the selector scores every candidate");
 
@@ -526,7 +603,8 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
   if (int st = check_variant(*v, b->mats_h[m].k)) return st;
   std::vector<BItem> items;
   try {
-    make_items(b->mats_h[m], b->rowptr[m].data(), *v, grid_filling_cap(b, m, item_cap(*v, b->mats_h[m].k)), items);
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), (uint32_t)b->esize, *v,
+               grid_filling_cap(b, m, item_cap(*v, b->mats_h[m].pitch)), items);
   } catch (const std::bad_alloc &) {
     return SPARSEP_ENOMEM;
   }
@@ -633,6 +711,20 @@ int sparsep_batch_select(sparsep_batch *b, sparsep_selector *sel, float min_conf
     if (fallback) fallback[m] = fb;
   }
   return sparsep_batch_commit(b);
+}
+
+// Committed work items by kind: window items (x tile staged) and chunks of
+// rows longer than one item.
+int sparsep_batch_item_kinds(const sparsep_batch *b, uint64_t *window_items, uint64_t *chunk_items) {
+  if (!b) return SPARSEP_EINVAL;
+  uint64_t w = 0, c = 0;
+  for (const BItem &it : b->items_h) {
+    if (it.mode == MODE_LONG) ++c;
+    else if (it.cw) ++w;
+  }
+  if (window_items) *window_items = w;
+  if (chunk_items) *chunk_items = c;
+  return SPARSEP_OK;
 }
 
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz) {

@@ -15,8 +15,17 @@ template <typename T> struct Mat {
   const T *val;
   const T *x;
   T *y;
-  uint32_t nrows, ncols, k, pad;
+  T *part;         // rows longer than BCAP: their chunks' partial rows (chunks x pitch each)
+  unsigned *cnt;   // and one arrival counter per such row (zero between launches)
+  uint32_t nrows, ncols, k;
+  uint32_t pitch;  // x / y row pitch in elements: k rounded up to a multiple of 4 (k >= 3)
 };
+
+// Row pitch of x and y on the device: k for k <= 2, else k rounded up to a
+// multiple of 4, so that every row starts on a 16-byte boundary and 4-wide
+// loads serve any k.  Column j of y depends on column j of x only, so the
+// pad columns never reach a result.
+constexpr uint32_t row_pitch(uint32_t k) { return k <= 2 ? k : (k + 3) & ~3u; }
 
 constexpr int BT = 256;            // threads per CTA
 constexpr uint32_t BCAP = 4096;    // nonzeros staged per item (and per long-row chunk)
@@ -24,6 +33,25 @@ constexpr uint32_t BRCAP = 1024;   // rows per item
 constexpr int ACC_REGS = 8;        // V * ACC accumulators per lane
 
 enum : uint8_t { MODE_ROWS = 0, MODE_MERGE = 1, MODE_LONG = 2 };
+
+// Per-CTA staging arena (static shared memory, under the 48 KB static limit
+// with the carry rows and the barrier).  A work item's staged arrays are
+// carved from it in this order, each region 16-byte aligned with room for the
+// alignment lead and tail of its copy: rowptr slice, column indices, values,
+// and for a window item the rows [c0, c0 + cw) of x.  The host cuts items so
+// that the carve fits; the kernel recomputes it from the item.
+constexpr uint32_t ARENA = 48000;
+struct Carve {
+  uint32_t col, val, xw, end;  // byte offsets (the rowptr slice starts at 0)
+};
+__host__ __device__ constexpr uint32_t align16(uint32_t v) { return (v + 15u) & ~15u; }
+__host__ __device__ constexpr Carve carve(uint32_t nr, uint32_t n, uint32_t es, uint32_t xbytes) {
+  return Carve{align16((nr + 1) * 4 + 32), align16((nr + 1) * 4 + 32) + align16(n * 4 + 32),
+               align16((nr + 1) * 4 + 32) + align16(n * 4 + 32) + align16(n * es + 32),
+               align16((nr + 1) * 4 + 32) + align16(n * 4 + 32) + align16(n * es + 32) +
+                   (xbytes ? align16(xbytes + 32) : 0)};
+}
+static_assert(carve(BRCAP, BCAP, 4, 0).end <= ARENA, "a full item of 4-byte values fits the arena");
 
 // A work item carries its matrix's arrays, so a CTA needs one load to start.
 struct BItem {
@@ -36,10 +64,16 @@ struct BItem {
   uint32_t p0, p1;  // nonzeros [p0, p1) = rowptr[r0] .. rowptr[r0 + nr]
   uint32_t ncols;   // columns of the matrix (bounds of x)
   uint16_t nr;      // rows (<= BRCAP)
-  uint16_t k;       // right-hand sides (x: ncols x k, y: nrows x k, row-major)
+  uint16_t k;       // row pitch of x (ncols x k) and y (nrows x k), row-major: the
+                    // right-hand sides rounded up (row_pitch), all computed
   uint8_t mode, lanes, vec, acc;
+  uint32_t c0;      // window item: x rows [c0, c0 + cw) staged in shared memory
+  uint32_t cw;      // and every column of the item inside them; 0: x read from memory.
+                    // MODE_LONG (one chunk of a row longer than BCAP): chunk c0 of cw
+  void *part;       // MODE_LONG: the row's chunk partials (cw x k elements)
+  unsigned *cnt;    // MODE_LONG: the row's arrival counter (the last chunk sums, resets)
 };
-static_assert(sizeof(BItem) == 64, "item layout");
+static_assert(sizeof(BItem) == 88, "item layout");
 
 // One kernel launch over items: with `head`, n CTAs claim items
 // items[0 .. n) in queue order by atomic ticket (head must be 0 at launch);

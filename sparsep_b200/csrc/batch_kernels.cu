@@ -4,56 +4,77 @@
 // A work item is a row range of one matrix holding at most BCAP nonzeros (or
 // one longer row, processed in BCAP-sized chunks), and carries that matrix's
 // array pointers.  A CTA runs one item: one thread issues TMA bulk copies of
-// the item's rowptr slice, column indices and values into shared memory
-// (16-byte aligned windows, completion on an mbarrier with a bounded wait),
-// so the whole item arrives in one memory round trip; afterwards only the x
-// gathers go to memory.  In the batch launch, CTAs claim items from a global
-// counter (atomicAdd, no waiting) in queue order -- long rows first -- so
-// matrices of very different sizes share the GPU without per-matrix launch
+// the item's rowptr slice, column indices and values into the CTA's staging
+// arena (16-byte aligned windows, completion on an mbarrier with a bounded
+// wait), so the whole item arrives in one memory round trip; afterwards only
+// the x gathers go to memory.  A window item (a 2D tile: a row range whose
+// columns all fall in a narrow range [c0, c0 + cw), as in banded matrices)
+// also stages those rows of x by the same bulk copy, and every gather of the
+// item is a shared-memory load.  In the batch launch, CTAs claim items from a
+// global counter (atomicAdd, no waiting) in queue order -- long rows first --
+// so matrices of very different sizes share the GPU without per-matrix launch
 // gaps or tails.
+//
+// x and y rows are `pitch` elements apart (k rounded up to a multiple of 4
+// for k >= 3), so every row starts on a 16-byte boundary and 4-wide loads
+// serve any k; the routines compute the whole padded row.
 //
 // Row routines, chosen per matrix (the autotuner picks among them).  The CTA
 // is cut into groups of G lanes; lane l of a group reads right-hand sides
 // [(l + aG)V, (l + aG)V + V) of each nonzero's x row with one V-wide load
-// (V in 1, 2, 4; k % V == 0), a < ACC, V * ACC <= 8 accumulators.
+// (V in 1, 2, 4; pitch % V == 0), a < ACC, V * ACC <= 8 accumulators.
 //   Rows mode: the item's rows dealt round-robin to the groups.
 //   Merge mode: the item's row ends and nonzeros split evenly over the groups
 //     along the merge path; rows cut by a split are finished from the
 //     groups' carries, in group order.
-//   Long rows (> BCAP nonzeros): the whole CTA, groups of G lanes striding
-//     over each staged chunk, then a fixed-order reduction over the groups.
+//   Long rows (> BCAP nonzeros): one item per BCAP-nonzero chunk, the CTA's
+//     groups on contiguous parts of it; partial rows summed in chunk order
+//     by the row's last chunk to arrive.
 // Same arithmetic as the single-vector path: integers accumulate in 32-bit
 // unsigned and wrap exactly; FP in the element type, each row's products
 // summed in a fixed order (deterministic from run to run).
 #include "batch.hpp"
 #include "device.cuh"
 
+// Registers of x in flight per lane (U nonzeros x V x ACC per step) and CTAs
+// per SM the register budget is set for.  Measured on the 512-matrix FP32
+// batch (autotuned queue): 16 / 4 CTAs 7.74 ms; 32 / 4 CTAs 7.79 ms (spills);
+// 32 / 3 CTAs 8.77 ms; the next step's loads issued before the current
+// step's products (software pipelining) 10.1-10.3 ms (spills).
+#ifndef SPARSEP_BATCH_XREGS
+#define SPARSEP_BATCH_XREGS 16
+#endif
+#ifndef SPARSEP_BATCH_MINB
+#define SPARSEP_BATCH_MINB 4
+#endif
+// Staged column indices and values read 4 (or 2) per shared load.
+#ifndef SPARSEP_BATCH_VLDS
+#define SPARSEP_BATCH_VLDS 0
+#endif
+
 namespace sparsep {
 namespace batch {
 
-constexpr uint32_t RP_N = BRCAP + 16;  // staged rowptr window (+ alignment lead and tail)
-constexpr uint32_t NZ_N = BCAP + 8;    // staged colind / values window
-
 template <typename T> struct BShared {
-  alignas(16) uint32_t rp[RP_N];
-  alignas(16) uint32_t col[NZ_N];  // after the compute: carries / long-row partials (<= BCAP accumulators)
-  alignas(16) T val[NZ_N];
+  alignas(16) unsigned char arena[ARENA];  // staged item (carve); after the compute: carries / partials
+  uint32_t crow[BT];                       // merge mode: the row each group left open
   alignas(8) uint64_t bar;
   unsigned next;
 };
 
-// The item's matrix, typed.
+// The item's matrix, typed.  x is global memory, or the staged window of a
+// window item (rows rebased to c0).
 template <typename T> struct View {
   const T *x;
   T *y;
-  uint32_t k;
+  uint32_t k;  // row pitch of x and y, all computed
   uint32_t ncols;
 };
 
 // The staged arrays, indexed from the item's first row / nonzero.
 template <typename T> struct Staged {
   const uint32_t *rp;  // rp[i] = rowptr[r0 + i]
-  const uint32_t *col; // col[q] = colind[p0 + q]
+  const uint32_t *col; // col[q] = colind[p0 + q] (window items: - c0)
   const T *val;
   uint32_t n;          // staged nonzeros
   int *err;
@@ -62,51 +83,42 @@ template <typename T> struct Staged {
 // Index guards: a failed check records its site code in the error word
 // (read by sparsep_batch_status) and the guarded work is skipped, so a
 // corrupted item or column index cannot take the GPU down.  The per-item ones
-// (staging windows, staged rowptr ends, every staged column inside x) are
-// always on; the checked build (-DSPARSEP_CHECK) adds a full scan of each
-// staged rowptr slice.
+// (staging windows, staged rowptr ends, every staged column inside x or the
+// window) are always on; the checked build (-DSPARSEP_CHECK) adds a full scan
+// of each staged rowptr slice.
 __device__ __forceinline__ bool bchk(bool ok, int *err, int code) {
   if (!ok && err) atomicCAS(err, 0, code);
   return ok;
 }
 
-template <typename T, int V> struct VecT;
-template <typename T> struct VecT<T, 1> {
-  T v[1];
-  static __device__ __forceinline__ VecT load(const T *p) {
-    VecT r;
-    r.v[0] = __ldg(p);
-    return r;
-  }
+template <typename T> __device__ __forceinline__ T bits_as(int v);
+template <> __device__ __forceinline__ float bits_as<float>(int v) { return __int_as_float(v); }
+template <> __device__ __forceinline__ int32_t bits_as<int32_t>(int v) { return v; }
+
+// V consecutive elements of x: read-only cache loads from global memory, or
+// shared-memory loads from a staged window (XS).
+template <typename T, int V> struct VecT {
+  T v[V];
 };
-template <typename T> struct VecT<T, 2> {
-  T v[2];
-  static __device__ __forceinline__ VecT load(const T *p) {
-    VecT r;
-    if constexpr (std::is_same<T, float>::value) {
-      const float2 q = __ldg(reinterpret_cast<const float2 *>(p));
-      r.v[0] = q.x, r.v[1] = q.y;
-    } else {
-      const int2 q = __ldg(reinterpret_cast<const int2 *>(p));
-      r.v[0] = (T)q.x, r.v[1] = (T)q.y;
-    }
-    return r;
+template <typename T, int V, bool XS> __device__ __forceinline__ VecT<T, V> ldx(const T *p) {
+  VecT<T, V> r;
+  if constexpr (V == 4) {
+    int4 q;
+    if constexpr (XS) q = *reinterpret_cast<const int4 *>(p);
+    else q = __ldg(reinterpret_cast<const int4 *>(p));
+    r.v[0] = bits_as<T>(q.x), r.v[1] = bits_as<T>(q.y), r.v[2] = bits_as<T>(q.z),
+    r.v[3] = bits_as<T>(q.w);
+  } else if constexpr (V == 2) {
+    int2 q;
+    if constexpr (XS) q = *reinterpret_cast<const int2 *>(p);
+    else q = __ldg(reinterpret_cast<const int2 *>(p));
+    r.v[0] = bits_as<T>(q.x), r.v[1] = bits_as<T>(q.y);
+  } else {
+    if constexpr (XS) r.v[0] = *p;
+    else r.v[0] = __ldg(p);
   }
-};
-template <typename T> struct VecT<T, 4> {
-  T v[4];
-  static __device__ __forceinline__ VecT load(const T *p) {
-    VecT r;
-    if constexpr (std::is_same<T, float>::value) {
-      const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
-      r.v[0] = q.x, r.v[1] = q.y, r.v[2] = q.z, r.v[3] = q.w;
-    } else {
-      const int4 q = __ldg(reinterpret_cast<const int4 *>(p));
-      r.v[0] = (T)q.x, r.v[1] = (T)q.y, r.v[2] = (T)q.z, r.v[3] = (T)q.w;
-    }
-    return r;
-  }
-};
+  return r;
+}
 
 template <typename T, int V> __device__ __forceinline__ void store_vec(T *p, const Acc<T> *a) {
   if constexpr (V == 4 && std::is_same<T, float>::value) {
@@ -136,7 +148,7 @@ __device__ __forceinline__ Window window(const void *base, uint64_t lo, uint64_t
   const uintptr_t b = reinterpret_cast<uintptr_t>(base) + hi * es;
   Window w;
   w.g0 = a & ~(uintptr_t)15;
-  w.bytes = (uint32_t)(((b + 15) & ~(uintptr_t)15) - w.g0);
+  w.bytes = lo < hi ? (uint32_t)(((b + 15) & ~(uintptr_t)15) - w.g0) : 0;
   w.lead = (uint32_t)((a - w.g0) / es);
   return w;
 }
@@ -150,17 +162,16 @@ __device__ __forceinline__ void bulk_copy(void *dst, uintptr_t src, uint32_t byt
       : "memory");
 }
 
-// Thread 0 arms the barrier for the windows' bytes and issues the copies.
-__device__ __forceinline__ void issue(uint64_t *bar, void *d0, const Window &w0, void *d1, const Window &w1,
-                                      void *d2, const Window &w2) {
+// Thread 0 arms the barrier for the windows' bytes and issues the copies
+// (up to four: rowptr, columns, values, x window).
+__device__ __forceinline__ void issue(uint64_t *bar, void *const (&dst)[4], const Window (&w)[4]) {
   // order earlier generic reads of the buffers before the async writes
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(w0.bytes + w1.bytes + w2.bytes)
+               "r"(w[0].bytes + w[1].bytes + w[2].bytes + w[3].bytes)
                : "memory");
-  bulk_copy(d0, w0.g0, w0.bytes, bar);
-  bulk_copy(d1, w1.g0, w1.bytes, bar);
-  bulk_copy(d2, w2.g0, w2.bytes, bar);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) bulk_copy(dst[i], w[i].g0, w[i].bytes, bar);
 }
 
 // Bounded wait for the barrier phase; true (for every thread of the CTA) if
@@ -194,13 +205,23 @@ __device__ __forceinline__ bool landed(uint64_t *bar, uint32_t parity, int *err)
   return true;
 }
 
-// Every staged column index below ncols (and `ok` on every thread): the gather
-// loops read x without per-load checks.  One pass over the staged chunk, shared
-// by all lanes; the result is the same on every thread of the CTA.
-__device__ __forceinline__ bool staged_ok(const uint32_t *col, uint32_t n, uint32_t ncols, bool ok, int *err,
-                                          int code) {
+// Every staged column index inside x (below ncols), or for a window item
+// inside the window, rebased to it (col - c0 < cw, written back); and `ok` on
+// every thread.  The gather loops then read x without per-load checks.  One
+// pass over the staged chunk, shared by all lanes; the result is the same on
+// every thread of the CTA.
+__device__ __forceinline__ bool staged_ok(uint32_t *col, uint32_t n, uint32_t c0, uint32_t bound, bool rebase,
+                                          bool ok, int *err, int code) {
   bool cols = true;
-  for (uint32_t q = threadIdx.x; q < n; q += BT) cols &= col[q] < ncols;
+  if (rebase) {
+    for (uint32_t q = threadIdx.x; q < n; q += BT) {
+      const uint32_t c = col[q] - c0;
+      cols &= c < bound;
+      col[q] = c;
+    }
+  } else {
+    for (uint32_t q = threadIdx.x; q < n; q += BT) cols &= col[q] < bound;
+  }
   ok = ok && bchk(cols, err, code);
   return !__syncthreads_or(!ok);
 }
@@ -215,75 +236,128 @@ template <typename T, int V, int ACC> __device__ __forceinline__ void zero_acc(A
     for (int u = 0; u < V; ++u) acc[a][u] = Acc<T>(0);
 }
 
-// Staged nonzeros [q, e) into the accumulators, in index order.  U nonzeros
-// per step, U * V * ACC = 16 registers of x in flight per lane.
-template <typename T, int G, int V, int ACC>
-__device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const View<T> &m, const Staged<T> &s, uint32_t q,
-                                          uint32_t e, int gl) {
-  constexpr int U = 16 / (V * ACC) > 2 ? 16 / (V * ACC) : 2;
-  const uint32_t k = m.k;
+// Accumulators of lane gl that fall inside the row: (gl + a G) V < k for a < na.
+template <int G, int V, int ACC> __device__ __forceinline__ int active_acc(int gl, uint32_t k) {
+  int na = 0;
+#pragma unroll
+  for (int a = 0; a < ACC; ++a) na += (uint32_t)(gl + a * G) * V < k;
+  return na;
+}
+
+// x row c of the view, from the lane's first column on: 64-bit offsets into
+// global memory, 32-bit into a staged window.
+template <typename T, bool XS> __device__ __forceinline__ const T *xrow(const T *xl, uint32_t c, uint32_t k) {
+  if constexpr (XS) return xl + c * k;
+  else return xl + (size_t)c * k;
+}
+
+// One staged nonzero into the accumulators.
+template <typename T, int G, int V, int ACC, bool XS>
+__device__ __forceinline__ void one_nz(Acc<T> (&acc)[ACC][V], const T *xl, uint32_t k, int na, const Staged<T> &s,
+                                       uint32_t q) {
+  const T *p = xrow<T, XS>(xl, s.col[q], k);
+  const T v = s.val[q];
+#pragma unroll
+  for (int a = 0; a < ACC; ++a)
+    if (a < na) {
+      const VecT<T, V> xv = ldx<T, V, XS>(p + a * G * V);
+#pragma unroll
+      for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v, xv.v[w]);
+    }
+}
+
+// W consecutive staged column indices and values (W-aligned in shared
+// memory) with one shared load each.
+template <typename T, int W>
+__device__ __forceinline__ void lds_vec(const uint32_t *col, const T *val, uint32_t *c, T *v) {
+  if constexpr (W == 4) {
+    uint32_t a0, a1, a2, a3, b0, b1, b2, b3;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3) : "r"(smem_u32(col)));
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(b0), "=r"(b1), "=r"(b2), "=r"(b3) : "r"(smem_u32(val)));
+    c[0] = a0, c[1] = a1, c[2] = a2, c[3] = a3;
+    v[0] = bits_as<T>((int)b0), v[1] = bits_as<T>((int)b1), v[2] = bits_as<T>((int)b2), v[3] = bits_as<T>((int)b3);
+  } else {
+    static_assert(W == 2, "2 or 4 per load");
+    uint32_t a0, a1, b0, b1;
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(a0), "=r"(a1) : "r"(smem_u32(col)));
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(b0), "=r"(b1) : "r"(smem_u32(val)));
+    c[0] = a0, c[1] = a1;
+    v[0] = bits_as<T>((int)b0), v[1] = bits_as<T>((int)b1);
+  }
+}
+
+// Staged nonzeros [q, e) into the accumulators, in index order.  xl is x plus
+// the lane's first column (gl V); accumulator a reads columns a G V further.
+// U nonzeros per step, U * V * ACC = SPARSEP_BATCH_XREGS registers of x in
+// flight per lane.
+template <typename T, int G, int V, int ACC, bool XS>
+__device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const T *xl, uint32_t k, int na,
+                                          const Staged<T> &s, uint32_t q, uint32_t e) {
+  constexpr int U = SPARSEP_BATCH_XREGS / (V * ACC) > 2 ? SPARSEP_BATCH_XREGS / (V * ACC) : 2;
   if (!bchk(q <= e && e <= s.n, s.err, -2101)) return;  // staged columns were checked against x once
+#if SPARSEP_BATCH_VLDS
+  // staged indices and values W at a time (one shared load each) from a
+  // W-aligned index on: the first nonzeros up to it go through the tail step
+  constexpr int W = U >= 4 ? 4 : U;
+  const uint32_t mis = (smem_u32(s.col + q) >> 2) & (W - 1);
+  const uint32_t peel = ((smem_u32(s.val + q) >> 2) & (W - 1)) == mis ? (W - mis) & (W - 1) : e - q;
+  for (const uint32_t stop = min(e, q + peel); q < stop; ++q) one_nz<T, G, V, ACC, XS>(acc, xl, k, na, s, q);
+#endif
   for (; q + U <= e; q += U) {
     uint32_t c[U];
     T v[U];
+#if SPARSEP_BATCH_VLDS
+#pragma unroll
+    for (int u = 0; u < U; u += W) lds_vec<T, W>(s.col + q + u, s.val + q + u, c + u, v + u);
+#else
 #pragma unroll
     for (int u = 0; u < U; ++u) c[u] = s.col[q + u], v[u] = s.val[q + u];
+#endif
     VecT<T, V> xv[U][ACC];
 #pragma unroll
-    for (int a = 0; a < ACC; ++a) {
-      const uint32_t j = (uint32_t)(gl + a * G) * V;
-      if (j < k)
+    for (int u = 0; u < U; ++u) {
+      const T *p = xrow<T, XS>(xl, c[u], k);
 #pragma unroll
-        for (int u = 0; u < U; ++u) xv[u][a] = VecT<T, V>::load(m.x + (size_t)c[u] * k + j);
+      for (int a = 0; a < ACC; ++a)
+        if (a < na) xv[u][a] = ldx<T, V, XS>(p + a * G * V);
     }
 #pragma unroll
-    for (int a = 0; a < ACC; ++a) {
-      const uint32_t j = (uint32_t)(gl + a * G) * V;
-      if (j < k)
+    for (int a = 0; a < ACC; ++a)
+      if (a < na)
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
           for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v[u], xv[u][a].v[w]);
-    }
   }
-  for (; q < e; ++q) {
-    const T *xr = m.x + (size_t)s.col[q] * k;
-    const T v = s.val[q];
-#pragma unroll
-    for (int a = 0; a < ACC; ++a) {
-      const uint32_t j = (uint32_t)(gl + a * G) * V;
-      if (j < k) {
-        const VecT<T, V> xv = VecT<T, V>::load(xr + j);
-#pragma unroll
-        for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v, xv.v[w]);
-      }
-    }
-  }
+  for (; q < e; ++q) one_nz<T, G, V, ACC, XS>(acc, xl, k, na, s, q);
 }
 
 template <typename T, int G, int V, int ACC>
-__device__ __forceinline__ void store_row(const View<T> &m, uint32_t row, Acc<T> (&acc)[ACC][V], int gl) {
-  T *yr = m.y + (size_t)row * m.k;
+__device__ __forceinline__ void store_row(T *yl, uint32_t row, uint32_t k, int na, Acc<T> (&acc)[ACC][V]) {
+  T *yr = yl + (size_t)row * k;
 #pragma unroll
-  for (int a = 0; a < ACC; ++a) {
-    const uint32_t j = (uint32_t)(gl + a * G) * V;
-    if (j < m.k) store_vec<T, V>(yr + j, acc[a]);
-  }
+  for (int a = 0; a < ACC; ++a)
+    if (a < na) store_vec<T, V>(yr + a * G * V, acc[a]);
 }
 
 // Rows mode: the item's rows dealt round-robin to groups of G lanes.
-template <typename T, int G, int V, int ACC>
+template <typename T, int G, int V, int ACC, bool XS>
 __device__ __forceinline__ void item_rows(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &,
                                           int tid) {
   using A = Acc<T>;
   constexpr int NG = BT / G;
   const int gi = tid / G, gl = tid % G;
+  const int na = active_acc<G, V, ACC>(gl, m.k);
+  const T *xl = m.x + gl * V;
+  T *yl = m.y + gl * V;
   const uint32_t nr = it.nr;
   for (uint32_t lr = gi; lr < nr; lr += NG) {
     A acc[ACC][V];
     zero_acc<T, V, ACC>(acc);
-    acc_range<T, G, V, ACC>(acc, m, s, s.rp[lr] - it.p0, s.rp[lr + 1] - it.p0, gl);
-    store_row<T, G, V, ACC>(m, it.r0 + lr, acc, gl);
+    acc_range<T, G, V, ACC, XS>(acc, xl, m.k, na, s, s.rp[lr] - it.p0, s.rp[lr + 1] - it.p0);
+    store_row<T, G, V, ACC>(yl, it.r0 + lr, m.k, na, acc);
   }
 }
 
@@ -307,13 +381,16 @@ __device__ __forceinline__ uint32_t merge_search(const uint32_t *rp, uint32_t p0
 // ends may have begun in earlier groups, so it waits for their carries (the
 // partial sums of the row each group left open) and adds them, earliest
 // first, to its own part.
-template <typename T, int G, int V, int ACC>
+template <typename T, int G, int V, int ACC, bool XS>
 __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
                                            int tid) {
   using A = Acc<T>;
   constexpr int NG = BT / G;
   const int gi = tid / G, gl = tid % G;
   const uint32_t k = m.k, nr = it.nr, n = it.p1 - it.p0, total = nr + n;
+  const int na = active_acc<G, V, ACC>(gl, k);
+  const T *xl = m.x + gl * V;
+  T *yl = m.y + gl * V;
   const uint32_t d0 = (uint32_t)((uint64_t)total * gi / NG), d1 = (uint32_t)((uint64_t)total * (gi + 1) / NG);
   const uint32_t i0 = merge_search(s.rp, it.p0, nr, n, d0), i1 = merge_search(s.rp, it.p0, nr, n, d1);
   const uint32_t j1 = d1 - i1;
@@ -324,7 +401,7 @@ __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s,
   for (uint32_t r = i0; r < i1; ++r) {
     const uint32_t e = s.rp[r + 1] - it.p0;
     zero_acc<T, V, ACC>(acc);
-    acc_range<T, G, V, ACC>(acc, m, s, j, e, gl);
+    acc_range<T, G, V, ACC, XS>(acc, xl, k, na, s, j, e);
     j = e;
     if (r == i0) {
 #pragma unroll
@@ -332,30 +409,28 @@ __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s,
 #pragma unroll
         for (int u = 0; u < V; ++u) head[a][u] = acc[a][u];
     } else {
-      store_row<T, G, V, ACC>(m, it.r0 + r, acc, gl);
+      store_row<T, G, V, ACC>(yl, it.r0 + r, k, na, acc);
     }
   }
   zero_acc<T, V, ACC>(acc);
-  acc_range<T, G, V, ACC>(acc, m, s, j, j1, gl);  // this group's part of row i1
-  __syncthreads();                                 // every group is done with the staged arrays
-  A *cbuf = reinterpret_cast<A *>(sh.col);         // NG * k <= BT * V * ACC <= BCAP partials
-  uint32_t *crow = sh.rp;                          // NG <= RP_N carry rows
+  acc_range<T, G, V, ACC, XS>(acc, xl, k, na, s, j, j1);  // this group's part of row i1
+  __syncthreads();                                         // every group is done with the staged arrays
+  A *cbuf = reinterpret_cast<A *>(sh.arena);               // NG * k <= BT * V * ACC partials
+  uint32_t *crow = sh.crow;
   if (gl == 0) crow[gi] = i1;
 #pragma unroll
-  for (int a = 0; a < ACC; ++a) {
-    const uint32_t jj = (uint32_t)(gl + a * G) * V;
-    if (jj < k)
+  for (int a = 0; a < ACC; ++a)
+    if (a < na)
 #pragma unroll
-      for (int u = 0; u < V; ++u) cbuf[gi * k + jj + u] = acc[a][u];
-  }
+      for (int u = 0; u < V; ++u) cbuf[gi * k + (gl + a * G) * V + u] = acc[a][u];
   __syncthreads();
   if (i0 < i1) {
     int g0 = gi;
     while (g0 > 0 && crow[g0 - 1] == i0) --g0;
 #pragma unroll
-    for (int a = 0; a < ACC; ++a) {
-      const uint32_t jj = (uint32_t)(gl + a * G) * V;
-      if (jj < k) {
+    for (int a = 0; a < ACC; ++a)
+      if (a < na) {
+        const uint32_t jj = (uint32_t)(gl + a * G) * V;
 #pragma unroll
         for (int u = 0; u < V; ++u) {
           A t = A(0);
@@ -363,108 +438,133 @@ __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s,
           head[a][u] = t + head[a][u];
         }
       }
-    }
-    store_row<T, G, V, ACC>(m, it.r0 + i0, head, gl);
+    store_row<T, G, V, ACC>(yl, it.r0 + i0, k, na, head);
   }
 }
 
-// One row longer than BCAP: chunks staged in turn, groups of G lanes stride
-// over each chunk's nonzeros, then the NG partial vectors are summed in group
-// order.  NG * k <= BT * ACC <= BCAP partials fit in the column buffer.
-template <typename T, int G, int ACC>
-__device__ __forceinline__ void item_long(const View<T> &m, const BItem &it, BShared<T> &sh, int tid, int *err) {
+// One chunk (<= BCAP nonzeros) of a row longer than BCAP; the row's chunks
+// are separate items, so a long row spreads over many SMs.  The CTA's groups
+// split the chunk's nonzeros into contiguous ranges (the row routines' vector
+// loads), their partial vectors are summed in group order into the chunk's
+// partial row, and the last of the row's chunks to arrive sums the partials
+// in chunk order into y (deterministic) and resets the row's counter.  Every
+// chunk arrives -- after a failed staging or check with a zero partial, the
+// error word set -- so the counter is zero again after every launch.
+template <typename T, int G, int V, int ACC>
+__device__ __forceinline__ void item_chunk(const BItem &it, BShared<T> &sh, int tid, int *err) {
   using A = Acc<T>;
   constexpr int NG = BT / G;
+  constexpr Carve cv = carve(0, BCAP, sizeof(T), 0);
+  const uint32_t k = it.k, n = it.p1 - it.p0;
   const int gi = tid / G, gl = tid % G;
-  const uint32_t k = m.k;
-  A acc[ACC][1];
-  zero_acc<T, 1, ACC>(acc);
-  uint32_t parity = 0;
-  for (uint32_t c0 = it.p0; c0 < it.p1; c0 += BCAP, parity ^= 1u) {
-    const uint32_t n = min(BCAP, it.p1 - c0);
-    const Window wc = window(it.colind, c0, c0 + n, 4), wv = window(it.val, c0, c0 + n, sizeof(T));
-    if (!bchk(wc.bytes <= sizeof(sh.col) && wv.bytes <= sizeof(sh.val), err, -2103)) return;
-    __syncthreads();  // the previous chunk is consumed
-    if (tid == 0) issue(&sh.bar, sh.col, wc, sh.val, wv, nullptr, Window{0, 0, 0});
-    if (!landed(&sh.bar, parity, err)) return;
-    const Staged<T> s{nullptr, sh.col + wc.lead, sh.val + wv.lead, n, err};
-    if (!staged_ok(s.col, n, m.ncols, true, err, -2107)) return;
-    for (uint32_t q = gi; q < n; q += NG) {
-      const T *xr = m.x + (size_t)s.col[q] * k;
-      const T v = s.val[q];
-#pragma unroll
-      for (int a = 0; a < ACC; ++a) {
-        const uint32_t j = (uint32_t)(gl + a * G);
-        if (j < k) acc[a][0] += mul<T>(v, __ldg(xr + j));
-      }
-    }
+  const int na = active_acc<G, V, ACC>(gl, k);
+  const Window w[4] = {window(it.colind, it.p0, it.p1, 4), window(it.val, it.p0, it.p1, sizeof(T)),
+                       Window{0, 0, 0}, Window{0, 0, 0}};
+  bool ok = bchk(n <= BCAP && it.c0 < it.cw && w[0].bytes <= cv.val - cv.col && w[1].bytes <= cv.xw - cv.val &&
+                     (uint32_t)NG * k * (uint32_t)sizeof(A) <= ARENA,
+                 err, -2103);
+  if (ok) {
+    void *const dst[4] = {sh.arena + cv.col, sh.arena + cv.val, nullptr, nullptr};
+    if (tid == 0) issue(&sh.bar, dst, w);
+    ok = landed(&sh.bar, 0, err);
   }
-  __syncthreads();
-  A *red = reinterpret_cast<A *>(sh.col);
-#pragma unroll
-  for (int a = 0; a < ACC; ++a) {
-    const uint32_t j = (uint32_t)(gl + a * G);
-    if (j < k) red[gi * k + j] = acc[a][0];
+  uint32_t *col = reinterpret_cast<uint32_t *>(sh.arena + cv.col) + w[0].lead;
+  if (ok) ok = staged_ok(col, n, 0, it.ncols, false, true, err, -2107);
+  A acc[ACC][V];
+  zero_acc<T, V, ACC>(acc);
+  if (ok) {
+    const Staged<T> s{nullptr, col, reinterpret_cast<const T *>(sh.arena + cv.val) + w[1].lead, n, err};
+    const uint32_t q0 = (uint32_t)((uint64_t)n * gi / NG), q1 = (uint32_t)((uint64_t)n * (gi + 1) / NG);
+    acc_range<T, G, V, ACC, false>(acc, static_cast<const T *>(it.x) + gl * V, k, na, s, q0, q1);
   }
+  __syncthreads();  // the staged chunk is consumed
+  A *red = reinterpret_cast<A *>(sh.arena);
+  if (ok)
+#pragma unroll
+    for (int a = 0; a < ACC; ++a)
+      if (a < na)
+#pragma unroll
+        for (int u = 0; u < V; ++u) red[gi * k + (gl + a * G) * V + u] = acc[a][u];
   __syncthreads();
-  T *yr = m.y + (size_t)it.r0 * k;
+  T *part = static_cast<T *>(it.part);
   for (uint32_t j = tid; j < k; j += BT) {
     A t = A(0);
-    for (int g = 0; g < NG; ++g) t += red[g * k + j];
+    if (ok)
+      for (int g = 0; g < NG; ++g) t += red[g * k + j];
+    part[(size_t)it.c0 * k + j] = from_acc<T>(t);
+  }
+  __threadfence();  // the partial is visible before the arrival
+  __syncthreads();
+  if (tid == 0) sh.next = atomicAdd(it.cnt, 1u) == it.cw - 1;
+  __syncthreads();
+  if (!sh.next) return;
+  __threadfence();
+  T *yr = static_cast<T *>(it.y) + (size_t)it.r0 * k;
+  for (uint32_t j = tid; j < k; j += BT) {
+    A t = A(0);
+    for (uint32_t c = 0; c < it.cw; ++c) t += A(__ldcg(part + (size_t)c * k + j));
     yr[j] = from_acc<T>(t);
   }
-}
-
-// ---------------------------------------------------------------------------
-// Dispatch on the item's (mode, lanes, vec, acc)
-// ---------------------------------------------------------------------------
-template <typename T, int MODE, int G, int V, int ACC>
-__device__ __forceinline__ void body(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh, int tid) {
-  if constexpr (MODE == MODE_ROWS) item_rows<T, G, V, ACC>(m, s, it, sh, tid);
-  else item_merge<T, G, V, ACC>(m, s, it, sh, tid);
-}
-
-template <typename T, int MODE, int G, int V>
-__device__ __forceinline__ void by_acc(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
-                                       int tid) {
-  switch (it.acc) {
-    case 1: body<T, MODE, G, V, 1>(m, s, it, sh, tid); break;
-    case 2: if constexpr (V <= 4) body<T, MODE, G, V, 2>(m, s, it, sh, tid); break;
-    case 4: if constexpr (V <= 2) body<T, MODE, G, V, 4>(m, s, it, sh, tid); break;
-    default: if constexpr (V == 1) body<T, MODE, G, V, 8>(m, s, it, sh, tid); break;
-  }
-}
-
-template <typename T, int MODE, int G>
-__device__ __forceinline__ void by_vec(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
-                                       int tid) {
-  switch (it.vec) {
-    case 4: by_acc<T, MODE, G, 4>(m, s, it, sh, tid); break;
-    case 2: by_acc<T, MODE, G, 2>(m, s, it, sh, tid); break;
-    default: by_acc<T, MODE, G, 1>(m, s, it, sh, tid); break;
-  }
-}
-
-template <typename T, int MODE>
-__device__ __forceinline__ void by_lanes(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
-                                         int tid) {
-  switch (it.lanes) {
-    case 1: by_vec<T, MODE, 1>(m, s, it, sh, tid); break;
-    case 2: by_vec<T, MODE, 2>(m, s, it, sh, tid); break;
-    case 4: by_vec<T, MODE, 4>(m, s, it, sh, tid); break;
-    case 8: by_vec<T, MODE, 8>(m, s, it, sh, tid); break;
-    case 16: by_vec<T, MODE, 16>(m, s, it, sh, tid); break;
-    default: by_vec<T, MODE, 32>(m, s, it, sh, tid); break;
-  }
+  if (tid == 0) atomicExch(it.cnt, 0u);
 }
 
 template <typename T, int G>
-__device__ __forceinline__ void long_acc(const View<T> &m, const BItem &it, BShared<T> &sh, int tid, int *err) {
+__device__ __forceinline__ void chunk_by_vec(const BItem &it, BShared<T> &sh, int tid, int *err) {
+  switch (it.vec) {
+    case 4:
+      if (it.acc == 2) item_chunk<T, G, 4, 2>(it, sh, tid, err);
+      else item_chunk<T, G, 4, 1>(it, sh, tid, err);
+      break;
+    case 2: item_chunk<T, G, 2, 1>(it, sh, tid, err); break;
+    default: item_chunk<T, G, 1, 1>(it, sh, tid, err); break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dispatch on the item's (mode, lanes, vec, acc) and whether x is staged.
+// Window items come from 4-wide variants only.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE, int G, int V, int ACC, bool XS>
+__device__ __forceinline__ void body(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh, int tid) {
+  if constexpr (MODE == MODE_ROWS) item_rows<T, G, V, ACC, XS>(m, s, it, sh, tid);
+  else item_merge<T, G, V, ACC, XS>(m, s, it, sh, tid);
+}
+
+template <typename T, int MODE, int G, int V, bool XS>
+__device__ __forceinline__ void by_acc(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
+                                       int tid) {
   switch (it.acc) {
-    case 1: item_long<T, G, 1>(m, it, sh, tid, err); break;
-    case 2: item_long<T, G, 2>(m, it, sh, tid, err); break;
-    case 4: item_long<T, G, 4>(m, it, sh, tid, err); break;
-    default: item_long<T, G, 8>(m, it, sh, tid, err); break;
+    case 1: body<T, MODE, G, V, 1, XS>(m, s, it, sh, tid); break;
+    case 2: if constexpr (V <= 4) body<T, MODE, G, V, 2, XS>(m, s, it, sh, tid); break;
+    case 4: if constexpr (V <= 2) body<T, MODE, G, V, 4, XS>(m, s, it, sh, tid); break;
+    default: if constexpr (V == 1) body<T, MODE, G, V, 8, XS>(m, s, it, sh, tid); break;
+  }
+}
+
+template <typename T, int MODE, int G, bool XS>
+__device__ __forceinline__ void by_vec(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
+                                       int tid) {
+  if constexpr (XS) {
+    by_acc<T, MODE, G, 4, XS>(m, s, it, sh, tid);
+  } else {
+    switch (it.vec) {
+      case 4: by_acc<T, MODE, G, 4, XS>(m, s, it, sh, tid); break;
+      case 2: by_acc<T, MODE, G, 2, XS>(m, s, it, sh, tid); break;
+      default: by_acc<T, MODE, G, 1, XS>(m, s, it, sh, tid); break;
+    }
+  }
+}
+
+template <typename T, int MODE, bool XS>
+__device__ __forceinline__ void by_lanes(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &sh,
+                                         int tid) {
+  switch (it.lanes) {
+    case 1: by_vec<T, MODE, 1, XS>(m, s, it, sh, tid); break;
+    case 2: by_vec<T, MODE, 2, XS>(m, s, it, sh, tid); break;
+    case 4: by_vec<T, MODE, 4, XS>(m, s, it, sh, tid); break;
+    case 8: by_vec<T, MODE, 8, XS>(m, s, it, sh, tid); break;
+    case 16: by_vec<T, MODE, 16, XS>(m, s, it, sh, tid); break;
+    default: by_vec<T, MODE, 32, XS>(m, s, it, sh, tid); break;
   }
 }
 
@@ -473,11 +573,11 @@ __device__ __forceinline__ void long_acc(const View<T> &m, const BItem &it, BSha
 // queue order (long rows first) whatever order the hardware schedules CTAs
 // in, and the block scheduler refills every SM as its CTAs finish.  (A loop
 // over items inside each CTA would keep the same order; it costs 128+
-// registers and spills across the ~100 inlined row routines, so each CTA
-// runs one.)  Without a ticket counter, CTA b runs item i0 + b (one matrix's
+// registers and spills across the inlined row routines, so each CTA runs
+// one.)  Without a ticket counter, CTA b runs item i0 + b (one matrix's
 // items: the per-matrix launches and the autotuner's timing runs).
 template <typename T>
-__global__ void __launch_bounds__(BT, 4) batch_items(const BItem *items, uint32_t i0, unsigned int *head, int *err) {
+__global__ void __launch_bounds__(BT, SPARSEP_BATCH_MINB) batch_items(const BItem *items, uint32_t i0, unsigned int *head, int *err) {
   __shared__ BShared<T> sh;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -487,39 +587,55 @@ __global__ void __launch_bounds__(BT, 4) batch_items(const BItem *items, uint32_
   }
   __syncthreads();
   const BItem it = items[head ? sh.next : i0 + blockIdx.x];
-  const View<T> m{static_cast<const T *>(it.x), static_cast<T *>(it.y), it.k, it.ncols};
   if (it.mode == MODE_LONG) {
     switch (it.lanes) {
-      case 1: long_acc<T, 1>(m, it, sh, tid, err); break;
-      case 2: long_acc<T, 2>(m, it, sh, tid, err); break;
-      case 4: long_acc<T, 4>(m, it, sh, tid, err); break;
-      case 8: long_acc<T, 8>(m, it, sh, tid, err); break;
-      case 16: long_acc<T, 16>(m, it, sh, tid, err); break;
-      default: long_acc<T, 32>(m, it, sh, tid, err); break;
+      case 1: chunk_by_vec<T, 1>(it, sh, tid, err); break;
+      case 2: chunk_by_vec<T, 2>(it, sh, tid, err); break;
+      case 4: chunk_by_vec<T, 4>(it, sh, tid, err); break;
+      case 8: chunk_by_vec<T, 8>(it, sh, tid, err); break;
+      case 16: chunk_by_vec<T, 16>(it, sh, tid, err); break;
+      default: chunk_by_vec<T, 32>(it, sh, tid, err); break;
     }
     return;
   }
-  const Window wr = window(it.rowptr, it.r0, it.r0 + it.nr + 1, 4);
-  const Window wc = window(it.colind, it.p0, it.p1, 4);
-  const Window wv = window(it.val, it.p0, it.p1, sizeof(T));
-  if (!bchk(wr.bytes <= sizeof(sh.rp) && wc.bytes <= sizeof(sh.col) && wv.bytes <= sizeof(sh.val) &&
-                it.nr <= BRCAP && it.p1 - it.p0 <= BCAP,
+  const uint32_t n = it.p1 - it.p0;
+  const bool win = it.cw != 0;
+  const Carve cv = carve(it.nr, n, sizeof(T), win ? it.cw * it.k * (uint32_t)sizeof(T) : 0);
+  const Window w[4] = {window(it.rowptr, it.r0, it.r0 + it.nr + 1, 4), window(it.colind, it.p0, it.p1, 4),
+                       window(it.val, it.p0, it.p1, sizeof(T)),
+                       win ? window(it.x, (uint64_t)it.c0 * it.k, (uint64_t)(it.c0 + it.cw) * it.k, sizeof(T))
+                           : Window{0, 0, 0}};
+  if (!bchk(it.nr <= BRCAP && n <= BCAP && cv.end <= ARENA && w[0].bytes <= cv.col &&
+                w[1].bytes <= cv.val - cv.col && w[2].bytes <= cv.xw - cv.val &&
+                (!win || (w[3].bytes <= cv.end - cv.xw && w[3].lead == 0 && it.vec == 4 &&
+                          (uint64_t)it.c0 + it.cw <= it.ncols)),
             err, -2104))
     return;
-  if (tid == 0) issue(&sh.bar, sh.rp, wr, sh.col, wc, sh.val, wv);
+  void *const dst[4] = {sh.arena, sh.arena + cv.col, sh.arena + cv.val, sh.arena + cv.xw};
+  if (tid == 0) issue(&sh.bar, dst, w);
   if (!landed(&sh.bar, 0, err)) return;
-  const Staged<T> s{sh.rp + wr.lead, sh.col + wc.lead, sh.val + wv.lead, it.p1 - it.p0, err};
+  uint32_t *col = reinterpret_cast<uint32_t *>(sh.arena + cv.col) + w[1].lead;
+  const Staged<T> s{reinterpret_cast<const uint32_t *>(sh.arena) + w[0].lead, col,
+                    reinterpret_cast<const T *>(sh.arena + cv.val) + w[2].lead, n, err};
   {
     // the staged rowptr must run from p0 to p1 (checked build: non-decreasing),
-    // and every staged column must lie inside x
+    // and every staged column must lie inside x (window items: inside the
+    // window, rebased to it)
     bool rp_ok = s.rp[0] == it.p0 && s.rp[it.nr] == it.p1;
 #ifdef SPARSEP_CHECK
     for (uint32_t i = tid; i < it.nr; i += BT) rp_ok = rp_ok && s.rp[i] <= s.rp[i + 1];
 #endif
-    if (!staged_ok(s.col, it.p1 - it.p0, it.ncols, bchk(rp_ok, err, -2105), err, -2106)) return;
+    if (!staged_ok(col, n, it.c0, win ? it.cw : it.ncols, win, bchk(rp_ok, err, -2105), err, -2106)) return;
   }
-  if (it.mode == MODE_ROWS) by_lanes<T, MODE_ROWS>(m, s, it, sh, tid);
-  else by_lanes<T, MODE_MERGE>(m, s, it, sh, tid);
+  if (win) {
+    const View<T> m{reinterpret_cast<const T *>(sh.arena + cv.xw), static_cast<T *>(it.y), it.k, it.cw};
+    if (it.mode == MODE_ROWS) by_lanes<T, MODE_ROWS, true>(m, s, it, sh, tid);
+    else by_lanes<T, MODE_MERGE, true>(m, s, it, sh, tid);
+  } else {
+    const View<T> m{static_cast<const T *>(it.x), static_cast<T *>(it.y), it.k, it.ncols};
+    if (it.mode == MODE_ROWS) by_lanes<T, MODE_ROWS, false>(m, s, it, sh, tid);
+    else by_lanes<T, MODE_MERGE, false>(m, s, it, sh, tid);
+  }
 }
 
 template <typename T>

@@ -1726,17 +1726,20 @@ static int run_t(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s, un
 // A multi-RHS plan on device buffers: x into the batch, one launch, y out
 // (stream-ordered on s; on the legacy stream, synchronous around the batch's
 // own stream).
+// The batch's rows are `pitch` elements apart, the caller's k: 2D copies.
 static int run_multi(sparsep_plan *p, const void *d_x, void *d_y, cudaStream_t s) {
-  const size_t xb = (size_t)p->ncols * p->nrhs * p->esize, yb = (size_t)p->nrows * p->nrhs * p->esize;
+  uint32_t pitch = 0;
+  if (int st = sparsep_batch_pitch(p->batch, 0, &pitch)) return st;
+  const size_t w = (size_t)p->nrhs * p->esize, pw = (size_t)pitch * p->esize;
   if (!s) {
-    if (d_x != p->xpad) CK(cudaMemcpy(p->xpad, d_x, xb, cudaMemcpyDeviceToDevice));
+    if (d_x != p->xpad) CK(cudaMemcpy2D(p->xpad, pw, d_x, w, w, p->ncols, cudaMemcpyDeviceToDevice));
     if (int st = sparsep_batch_execute(p->batch, nullptr)) return st;
-    if (d_y != p->y) CK(cudaMemcpy(d_y, p->y, yb, cudaMemcpyDeviceToDevice));
+    if (d_y != p->y) CK(cudaMemcpy2D(d_y, w, p->y, pw, w, p->nrows, cudaMemcpyDeviceToDevice));
     return SPARSEP_OK;
   }
-  if (d_x != p->xpad) CK(cudaMemcpyAsync(p->xpad, d_x, xb, cudaMemcpyDeviceToDevice, s));
+  if (d_x != p->xpad) CK(cudaMemcpy2DAsync(p->xpad, pw, d_x, w, w, p->ncols, cudaMemcpyDeviceToDevice, s));
   if (int st = sparsep_batch_execute(p->batch, s)) return st;
-  if (d_y != p->y) CK(cudaMemcpyAsync(d_y, p->y, yb, cudaMemcpyDeviceToDevice, s));
+  if (d_y != p->y) CK(cudaMemcpy2DAsync(d_y, w, p->y, pw, w, p->nrows, cudaMemcpyDeviceToDevice, s));
   return SPARSEP_OK;
 }
 

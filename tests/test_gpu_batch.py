@@ -115,3 +115,91 @@ def test_batch_wide_rhs(dtype):
         b.commit()
         b.execute()
         check_batch(b, mats, data, dtype)
+
+
+def long_row_batch(dtype, seed=11):
+    """Matrices whose longest rows exceed one 4096-nonzero chunk (4097 up to
+    50,000 nonzeros, so 2..13 chunk items per row) beside ordinary rows, with
+    k = 1, 3, 16 and 33 right-hand sides."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m, (k, long_lens) in enumerate(((1, (4097, 9000)), (3, (8192, 50000)), (16, (12289,)), (33, (4097, 20000)))):
+        n = 60_000
+        lens = rng.integers(1, 40, n)
+        rows = rng.choice(n, len(long_lens), replace=False)
+        lens[rows] = long_lens
+        rp = np.zeros(n + 1, dtype=np.uint32)
+        np.cumsum(lens, out=rp[1:])
+        ci = np.concatenate([np.sort(rng.choice(n, int(l), replace=False)) for l in lens]).astype(np.uint32)
+        np_t = capi.DTYPES[dtype].np
+        vv = (rng.uniform(-1, 1, ci.size) if dtype == "f32" else rng.integers(-8, 9, ci.size)).astype(np_t)
+        x = (rng.uniform(-1, 1, (n, k)) if dtype == "f32" else rng.integers(-8, 9, (n, k))).astype(np_t)
+        out.append((n, rp, ci, vv, k, x))
+    return out
+
+
+@pytest.mark.parametrize("dtype", ["f32", "i32"])
+def test_batch_long_rows(dtype):
+    """Rows longer than a chunk run as one item per chunk on many CTAs; the
+    last chunk to arrive sums the partial rows.  Results stay right over
+    repeated graph launches, per-matrix launches, every applicable candidate
+    and the autotuner's timing runs -- the rows' arrival counters return to
+    zero after every launch."""
+    data = long_row_batch(dtype)
+    mats = [sp.csr(dtype, n, n, rp, ci, vv) for (n, rp, ci, vv, k, x) in data]
+    b = sp.capi.Batch(dtype, mats, [d[4] for d in data])
+    for m, d in enumerate(data):
+        b.set_x(m, d[5])
+    assert b.item_kinds()[1] == sum(-(-int(l) // 4096) for d in data for l in np.diff(d[1].astype(np.int64))
+                                    if l > 4096)
+    for _ in range(3):
+        b.execute()
+        check_batch(b, mats, data, dtype)
+    b.execute_per_matrix()
+    check_batch(b, mats, data, dtype)
+    for v in sp.capi.batch_candidates()[::5]:
+        for m, d in enumerate(data):
+            if v.applies(d[4]):
+                b.set_variant(m, v)
+        b.commit()
+        b.execute()
+        check_batch(b, mats, data, dtype)
+    b.autotune(reps=1)
+    b.execute()
+    check_batch(b, mats, data, dtype)
+    b.status()
+
+
+@pytest.mark.parametrize("dtype", ["f32", "i32"])
+def test_batch_window_items(dtype):
+    """Banded matrices under the window variants: x tiles staged in shared
+    memory (including spans just inside and beyond what the arena holds, so
+    that window and ordinary items alternate), every column against the
+    oracle."""
+    rng = np.random.default_rng(12)
+    data = []
+    for m, (k, bw) in enumerate(((4, 8), (7, 64), (16, 200), (32, 90), (12, 1500))):
+        n = int(rng.integers(5_000, 20_000))
+        r = np.arange(n)
+        lo = np.maximum(0, r - bw)
+        hi = np.minimum(n, r + bw + 1)
+        lens = np.minimum(hi - lo, rng.integers(4, 65, n))
+        rp, ci = sp.synth.stratified_cols(rng, lens, lo, hi)
+        np_t = capi.DTYPES[dtype].np
+        vv = (rng.uniform(-1, 1, ci.size) if dtype == "f32" else rng.integers(-8, 9, ci.size)).astype(np_t)
+        x = (rng.uniform(-1, 1, (n, k)) if dtype == "f32" else rng.integers(-8, 9, (n, k))).astype(np_t)
+        data.append((n, rp, ci, vv, k, x))
+    mats = [sp.csr(dtype, n, n, rp, ci, vv) for (n, rp, ci, vv, k, x) in data]
+    b = sp.capi.Batch(dtype, mats, [d[4] for d in data])
+    for m, d in enumerate(data):
+        b.set_x(m, d[5])
+    for v in sp.capi.batch_candidates():
+        if not v.mode & 2 or not any(v.applies(d[4]) for d in data):
+            continue
+        for m, d in enumerate(data):
+            b.set_variant(m, v if v.applies(d[4]) else sp.capi.BatchVariant(1, 8, 0, 4))
+        b.commit()
+        nwin, _ = b.item_kinds()
+        assert nwin > 0
+        b.execute()
+        check_batch(b, mats, data, dtype)

@@ -268,11 +268,11 @@ HELDOUT_WIDE = selector.DATA / "heldout_wide.npz"
 @pytest.mark.gpu
 @pytest.mark.skipif(not (selector.MODEL.exists() and HELDOUT_WIDE.exists()), reason="no trained model committed")
 def test_trained_model_gain_on_wider_matrices():
-    """Held-out matrices outside the training range (rows 8k-2.1M, 2-128
-    nonzeros per row, up to 10 M nonzeros; the training set stops at 262k
-    rows and 64 per row), timed on a B200 by the autotuner: the network's
-    picks still run within 10% of the exhaustive best in total and beat the
-    default variant."""
+    """Held-out matrices of the wide range (rows 8k-2.1M, 2-128 nonzeros
+    per row, up to 10 M nonzeros; 2,000 of the 22,000 training matrices come
+    from that range, the rest from 1k-262k rows and 2-64 per row), timed on a
+    B200 by the autotuner: the network's picks run within 10% of the
+    exhaustive best in total and beat the default variant."""
     h = np.load(HELDOUT_WIDE)
     assert h["meta"][:, 1].max() > 1_000_000 and h["meta"][:, 2].max() > 4_000_000
     res = selector.evaluate(selector.selector(selector.load()).scores(h["feats"]), h["times"], h["meta"][:, 3])
