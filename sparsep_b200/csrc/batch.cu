@@ -217,8 +217,8 @@ extern "C" void sparsep_batch_variant_default(uint32_t nrhs, sparsep_batch_varia
   v->item_work = 0;
 }
 
-// Queue order of the batch launch: long-row items first (largest
-// first), then the rest matrix after matrix.
+// Queue order of the batch launch: long-row chunks first (rows with the most
+// chunks first), then the rest matrix after matrix.
 static void queue_order(const std::vector<BItem> &in, std::vector<BItem> &q) {
   q.clear();
   q.reserve(in.size());

@@ -28,7 +28,17 @@ template <typename T> struct Mat {
 constexpr uint32_t row_pitch(uint32_t k) { return k <= 2 ? k : (k + 3) & ~3u; }
 
 constexpr int BT = 256;            // threads per CTA
-constexpr uint32_t BCAP = 4096;    // nonzeros staged per item (and per long-row chunk)
+#ifndef SPARSEP_BATCH_BCAP
+#define SPARSEP_BATCH_BCAP 4096
+#endif
+#ifndef SPARSEP_BATCH_ARENA
+#define SPARSEP_BATCH_ARENA 48000
+#endif
+#ifndef SPARSEP_BATCH_MINB
+#define SPARSEP_BATCH_MINB 4
+#endif
+constexpr uint32_t MINB = SPARSEP_BATCH_MINB;  // CTAs per SM the kernel's registers are budgeted for
+constexpr uint32_t BCAP = SPARSEP_BATCH_BCAP;  // nonzeros staged per item (and per long-row chunk)
 constexpr uint32_t BRCAP = 1024;   // rows per item
 constexpr int ACC_REGS = 8;        // V * ACC accumulators per lane
 
@@ -40,7 +50,7 @@ enum : uint8_t { MODE_ROWS = 0, MODE_MERGE = 1, MODE_LONG = 2 };
 // alignment lead and tail of its copy: rowptr slice, column indices, values,
 // and for a window item the rows [c0, c0 + cw) of x.  The host cuts items so
 // that the carve fits; the kernel recomputes it from the item.
-constexpr uint32_t ARENA = 48000;
+constexpr uint32_t ARENA = SPARSEP_BATCH_ARENA;
 struct Carve {
   uint32_t col, val, xw, end;  // byte offsets (the rowptr slice starts at 0)
 };

@@ -36,20 +36,14 @@
 #include "batch.hpp"
 #include "device.cuh"
 
-// Registers of x in flight per lane (U nonzeros x V x ACC per step) and CTAs
-// per SM the register budget is set for.  Measured on the 512-matrix FP32
-// batch (autotuned queue): 16 / 4 CTAs 7.74 ms; 32 / 4 CTAs 7.79 ms (spills);
-// 32 / 3 CTAs 8.77 ms; the next step's loads issued before the current
-// step's products (software pipelining) 10.1-10.3 ms (spills).
+// Registers of x in flight per lane (U nonzeros x V x ACC per step), with the
+// register budget of MINB CTAs per SM.  Measured on the 512-matrix FP32
+// batch (autotuned queue, one run each): 16 / 4 CTAs 7.74 ms; 32 / 4 CTAs
+// 7.79 ms (spills); 32 / 3 CTAs 8.77 ms; 16 / 5 CTAs (48 registers) 7.60 ms;
+// the next step's loads issued before the current step's products (software
+// pipelining) 10.1-10.3 ms (spills).
 #ifndef SPARSEP_BATCH_XREGS
 #define SPARSEP_BATCH_XREGS 16
-#endif
-#ifndef SPARSEP_BATCH_MINB
-#define SPARSEP_BATCH_MINB 4
-#endif
-// Staged column indices and values read 4 (or 2) per shared load.
-#ifndef SPARSEP_BATCH_VLDS
-#define SPARSEP_BATCH_VLDS 0
 #endif
 
 namespace sparsep {
@@ -266,28 +260,6 @@ __device__ __forceinline__ void one_nz(Acc<T> (&acc)[ACC][V], const T *xl, uint3
     }
 }
 
-// W consecutive staged column indices and values (W-aligned in shared
-// memory) with one shared load each.
-template <typename T, int W>
-__device__ __forceinline__ void lds_vec(const uint32_t *col, const T *val, uint32_t *c, T *v) {
-  if constexpr (W == 4) {
-    uint32_t a0, a1, a2, a3, b0, b1, b2, b3;
-    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3) : "r"(smem_u32(col)));
-    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(b0), "=r"(b1), "=r"(b2), "=r"(b3) : "r"(smem_u32(val)));
-    c[0] = a0, c[1] = a1, c[2] = a2, c[3] = a3;
-    v[0] = bits_as<T>((int)b0), v[1] = bits_as<T>((int)b1), v[2] = bits_as<T>((int)b2), v[3] = bits_as<T>((int)b3);
-  } else {
-    static_assert(W == 2, "2 or 4 per load");
-    uint32_t a0, a1, b0, b1;
-    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(a0), "=r"(a1) : "r"(smem_u32(col)));
-    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(b0), "=r"(b1) : "r"(smem_u32(val)));
-    c[0] = a0, c[1] = a1;
-    v[0] = bits_as<T>((int)b0), v[1] = bits_as<T>((int)b1);
-  }
-}
-
 // Staged nonzeros [q, e) into the accumulators, in index order.  xl is x plus
 // the lane's first column (gl V); accumulator a reads columns a G V further.
 // U nonzeros per step, U * V * ACC = SPARSEP_BATCH_XREGS registers of x in
@@ -297,24 +269,11 @@ __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const T *xl, ui
                                           const Staged<T> &s, uint32_t q, uint32_t e) {
   constexpr int U = SPARSEP_BATCH_XREGS / (V * ACC) > 2 ? SPARSEP_BATCH_XREGS / (V * ACC) : 2;
   if (!bchk(q <= e && e <= s.n, s.err, -2101)) return;  // staged columns were checked against x once
-#if SPARSEP_BATCH_VLDS
-  // staged indices and values W at a time (one shared load each) from a
-  // W-aligned index on: the first nonzeros up to it go through the tail step
-  constexpr int W = U >= 4 ? 4 : U;
-  const uint32_t mis = (smem_u32(s.col + q) >> 2) & (W - 1);
-  const uint32_t peel = ((smem_u32(s.val + q) >> 2) & (W - 1)) == mis ? (W - mis) & (W - 1) : e - q;
-  for (const uint32_t stop = min(e, q + peel); q < stop; ++q) one_nz<T, G, V, ACC, XS>(acc, xl, k, na, s, q);
-#endif
   for (; q + U <= e; q += U) {
     uint32_t c[U];
     T v[U];
-#if SPARSEP_BATCH_VLDS
-#pragma unroll
-    for (int u = 0; u < U; u += W) lds_vec<T, W>(s.col + q + u, s.val + q + u, c + u, v + u);
-#else
 #pragma unroll
     for (int u = 0; u < U; ++u) c[u] = s.col[q + u], v[u] = s.val[q + u];
-#endif
     VecT<T, V> xv[U][ACC];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -577,7 +536,8 @@ __device__ __forceinline__ void by_lanes(const View<T> &m, const Staged<T> &s, c
 // one.)  Without a ticket counter, CTA b runs item i0 + b (one matrix's
 // items: the per-matrix launches and the autotuner's timing runs).
 template <typename T>
-__global__ void __launch_bounds__(BT, SPARSEP_BATCH_MINB) batch_items(const BItem *items, uint32_t i0, unsigned int *head, int *err) {
+__global__ void __launch_bounds__(BT, MINB)
+    batch_items(const BItem *items, uint32_t i0, unsigned int *head, int *err) {
   __shared__ BShared<T> sh;
   const int tid = threadIdx.x;
   if (tid == 0) {
