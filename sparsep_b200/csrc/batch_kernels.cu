@@ -23,10 +23,12 @@
 // is cut into groups of G lanes; lane l of a group reads right-hand sides
 // [(l + aG)V, (l + aG)V + V) of each nonzero's x row with one V-wide load
 // (V in 1, 2, 4; pitch % V == 0), a < ACC, V * ACC <= 8 accumulators.
-//   Rows mode: the item's rows dealt round-robin to the groups.
+//   Rows mode: the item's rows cut into one contiguous block per group.
 //   Merge mode: the item's row ends and nonzeros split evenly over the groups
 //     along the merge path; rows cut by a split are finished from the
 //     groups' carries, in group order.
+//   Either way a group streams its nonzeros in steps of U across row ends,
+//   so its loads stay U deep in flight rather than draining at every row.
 //   Long rows (> BCAP nonzeros): one item per BCAP-nonzero chunk, the CTA's
 //     groups on contiguous parts of it; partial rows summed in chunk order
 //     by the row's last chunk to arrive.
@@ -245,52 +247,42 @@ template <typename T, bool XS> __device__ __forceinline__ const T *xrow(const T 
   else return xl + (size_t)c * k;
 }
 
-// One staged nonzero into the accumulators.
-template <typename T, int G, int V, int ACC, bool XS>
-__device__ __forceinline__ void one_nz(Acc<T> (&acc)[ACC][V], const T *xl, uint32_t k, int na, const Staged<T> &s,
-                                       uint32_t q) {
-  const T *p = xrow<T, XS>(xl, s.col[q], k);
-  const T v = s.val[q];
-#pragma unroll
-  for (int a = 0; a < ACC; ++a)
-    if (a < na) {
-      const VecT<T, V> xv = ldx<T, V, XS>(p + a * G * V);
-#pragma unroll
-      for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v, xv.v[w]);
-    }
-}
-
 // Staged nonzeros [q, e) into the accumulators, in index order.  xl is x plus
 // the lane's first column (gl V); accumulator a reads columns a G V further.
 // U nonzeros per step, U * V * ACC = SPARSEP_BATCH_XREGS registers of x in
-// flight per lane.
+// flight per lane; the last e - q < U nonzeros as one masked step (one round
+// trip), products added in index order either way.
 template <typename T, int G, int V, int ACC, bool XS>
 __device__ __forceinline__ void acc_range(Acc<T> (&acc)[ACC][V], const T *xl, uint32_t k, int na,
                                           const Staged<T> &s, uint32_t q, uint32_t e) {
   constexpr int U = SPARSEP_BATCH_XREGS / (V * ACC) > 2 ? SPARSEP_BATCH_XREGS / (V * ACC) : 2;
   if (!bchk(q <= e && e <= s.n, s.err, -2101)) return;  // staged columns were checked against x once
-  for (; q + U <= e; q += U) {
+  for (; q < e; q += U) {
     uint32_t c[U];
     T v[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) c[u] = s.col[q + u], v[u] = s.val[q + u];
+    for (int u = 0; u < U; ++u) {
+      const bool in = q + u < e;
+      c[u] = in ? s.col[q + u] : 0u;
+      v[u] = in ? s.val[q + u] : T(0);
+    }
     VecT<T, V> xv[U][ACC];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const T *p = xrow<T, XS>(xl, c[u], k);
 #pragma unroll
       for (int a = 0; a < ACC; ++a)
-        if (a < na) xv[u][a] = ldx<T, V, XS>(p + a * G * V);
+        if (a < na && q + u < e) xv[u][a] = ldx<T, V, XS>(p + a * G * V);
     }
 #pragma unroll
     for (int a = 0; a < ACC; ++a)
       if (a < na)
 #pragma unroll
         for (int u = 0; u < U; ++u)
+          if (q + u < e)
 #pragma unroll
-          for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v[u], xv[u][a].v[w]);
+            for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v[u], xv[u][a].v[w]);
   }
-  for (; q < e; ++q) one_nz<T, G, V, ACC, XS>(acc, xl, k, na, s, q);
 }
 
 template <typename T, int G, int V, int ACC>
@@ -301,7 +293,66 @@ __device__ __forceinline__ void store_row(T *yl, uint32_t row, uint32_t k, int n
     if (a < na) store_vec<T, V>(yr + a * G * V, acc[a]);
 }
 
-// Rows mode: the item's rows dealt round-robin to groups of G lanes.
+// Item-local nonzeros [j, j1) of rows r .. i1 - 1 (row r may have begun
+// before j) and the start of row i1, in steps of U across row ends, so that U
+// loads stay in flight all along.  Each row is summed from zero in index
+// order; with keep_first, row r's sum goes to head (its earlier part is in
+// other groups' carries), every other finished row to y.  Returns with acc
+// holding this range's part of row i1 (zero when [j, j1) ends with row i1 - 1).
+template <typename T, int G, int V, int ACC, bool XS>
+__device__ __forceinline__ void stream_rows(Acc<T> (&acc)[ACC][V], Acc<T> (&head)[ACC][V], bool keep_first,
+                                            const T *xl, T *yl, uint32_t k, int na, const Staged<T> &s,
+                                            const BItem &it, uint32_t r, uint32_t i1, uint32_t j, uint32_t j1) {
+  const uint32_t first = r;
+  uint32_t rend = r < i1 ? s.rp[r + 1] - it.p0 : j1;
+  zero_acc<T, V, ACC>(acc);
+  auto finish = [&]() {
+    if (keep_first && r == first) {
+#pragma unroll
+      for (int a = 0; a < ACC; ++a)
+#pragma unroll
+        for (int u = 0; u < V; ++u) head[a][u] = acc[a][u];
+    } else {
+      store_row<T, G, V, ACC>(yl, it.r0 + r, k, na, acc);
+    }
+    zero_acc<T, V, ACC>(acc);
+    ++r;
+    rend = r < i1 ? s.rp[r + 1] - it.p0 : j1;
+  };
+  constexpr int U = SPARSEP_BATCH_XREGS / (V * ACC) > 2 ? SPARSEP_BATCH_XREGS / (V * ACC) : 2;
+  for (uint32_t q = j; q < j1; q += U) {
+    uint32_t c[U];
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool in = q + u < j1;
+      c[u] = in ? s.col[q + u] : 0u;
+      v[u] = in ? s.val[q + u] : T(0);
+    }
+    VecT<T, V> xv[U][ACC];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const T *p = xrow<T, XS>(xl, c[u], k);
+#pragma unroll
+      for (int a = 0; a < ACC; ++a)
+        if (a < na && q + u < j1) xv[u][a] = ldx<T, V, XS>(p + a * G * V);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (q + u < j1) {
+        while (r < i1 && rend == q + u) finish();  // rows ending here (empty ones too)
+#pragma unroll
+        for (int a = 0; a < ACC; ++a)
+          if (a < na)
+#pragma unroll
+            for (int w = 0; w < V; ++w) acc[a][w] += mul<T>(v[u], xv[u][a].v[w]);
+      }
+  }
+  while (r < i1) finish();  // rows ending at j1, all their nonzeros consumed
+}
+
+// Rows mode: the item's rows cut into NG contiguous blocks of whole rows, one
+// per group of G lanes, each streamed through; no carries.
 template <typename T, int G, int V, int ACC, bool XS>
 __device__ __forceinline__ void item_rows(const View<T> &m, const Staged<T> &s, const BItem &it, BShared<T> &,
                                           int tid) {
@@ -309,15 +360,11 @@ __device__ __forceinline__ void item_rows(const View<T> &m, const Staged<T> &s, 
   constexpr int NG = BT / G;
   const int gi = tid / G, gl = tid % G;
   const int na = active_acc<G, V, ACC>(gl, m.k);
-  const T *xl = m.x + gl * V;
-  T *yl = m.y + gl * V;
   const uint32_t nr = it.nr;
-  for (uint32_t lr = gi; lr < nr; lr += NG) {
-    A acc[ACC][V];
-    zero_acc<T, V, ACC>(acc);
-    acc_range<T, G, V, ACC, XS>(acc, xl, m.k, na, s, s.rp[lr] - it.p0, s.rp[lr + 1] - it.p0);
-    store_row<T, G, V, ACC>(yl, it.r0 + lr, m.k, na, acc);
-  }
+  const uint32_t ra = (uint32_t)((uint64_t)nr * gi / NG), rb = (uint32_t)((uint64_t)nr * (gi + 1) / NG);
+  A acc[ACC][V], head[ACC][V];
+  stream_rows<T, G, V, ACC, XS>(acc, head, false, m.x + gl * V, m.y + gl * V, m.k, na, s, it, ra, rb,
+                                s.rp[ra] - it.p0, s.rp[rb] - it.p0);
 }
 
 // Rows completed before merge-path diagonal d of the item's row ends
@@ -351,29 +398,18 @@ __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s,
   const T *xl = m.x + gl * V;
   T *yl = m.y + gl * V;
   const uint32_t d0 = (uint32_t)((uint64_t)total * gi / NG), d1 = (uint32_t)((uint64_t)total * (gi + 1) / NG);
-  const uint32_t i0 = merge_search(s.rp, it.p0, nr, n, d0), i1 = merge_search(s.rp, it.p0, nr, n, d1);
-  const uint32_t j1 = d1 - i1;
-  uint32_t j = d0 - i0;
-  bchk(i0 <= i1 && i1 <= nr && j <= j1 && j1 <= n, s.err, -2102);
+  const uint32_t i0 = merge_search(s.rp, it.p0, nr, n, d0);
+  uint32_t i1 = merge_search(s.rp, it.p0, nr, n, d1);
+  const uint32_t j = d0 - i0;
+  uint32_t j1 = d1 - i1;
+  // a failed check leaves the group's range empty (the error is recorded); the
+  // group still takes part in the barriers below
+  if (!bchk(i0 <= i1 && i1 <= nr && j <= j1 && j1 <= n, s.err, -2102)) i1 = i0, j1 = j;
   A head[ACC][V], acc[ACC][V];
   zero_acc<T, V, ACC>(head);
-  for (uint32_t r = i0; r < i1; ++r) {
-    const uint32_t e = s.rp[r + 1] - it.p0;
-    zero_acc<T, V, ACC>(acc);
-    acc_range<T, G, V, ACC, XS>(acc, xl, k, na, s, j, e);
-    j = e;
-    if (r == i0) {
-#pragma unroll
-      for (int a = 0; a < ACC; ++a)
-#pragma unroll
-        for (int u = 0; u < V; ++u) head[a][u] = acc[a][u];
-    } else {
-      store_row<T, G, V, ACC>(yl, it.r0 + r, k, na, acc);
-    }
-  }
-  zero_acc<T, V, ACC>(acc);
-  acc_range<T, G, V, ACC, XS>(acc, xl, k, na, s, j, j1);  // this group's part of row i1
-  __syncthreads();                                         // every group is done with the staged arrays
+  stream_rows<T, G, V, ACC, XS>(acc, head, true, xl, yl, k, na, s, it, i0, i1, j, j1);
+  // acc: this group's part of row i1
+  __syncthreads();  // every group is done with the staged arrays
   A *cbuf = reinterpret_cast<A *>(sh.arena);               // NG * k <= BT * V * ACC partials
   uint32_t *crow = sh.crow;
   if (gl == 0) crow[gi] = i1;

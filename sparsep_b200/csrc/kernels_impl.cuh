@@ -134,6 +134,10 @@ __device__ void csr_rows(const Params<T> &P, const Item &it, const T *__restrict
 // written with consecutive threads on consecutive rows.  A row longer than the
 // chunk capacity is reduced by the whole CTA straight from global memory.
 // ---------------------------------------------------------------------------
+// x gathers each thread keeps in flight in the chunk's product pass: 4 x this.
+#ifndef SPARSEP_CSR_GATHER
+#define SPARSEP_CSR_GATHER 1
+#endif
 constexpr int CSR_CAP = 4096;   // nonzeros per chunk
 constexpr int CSR_RCAP = 1024;  // rows per chunk
 constexpr int CSR_SHORT = 48;   // rows up to this length are summed by one thread
@@ -204,17 +208,43 @@ __device__ void csr_stream(const Params<T> &P, const Item &it, const T *__restri
       continue;
     }
     const uint64_t s0 = (uint64_t)base + it.nnz_base, e0 = (uint64_t)srp[k] + it.nnz_base;
-    for (uint64_t g = (s0 >> 2) + threadIdx.x; 4 * g < e0; g += blockDim.x) {
-      const uint64_t j = 4 * g;
-      if (SP_BAD(P, j + 3 < P.n_idx && j + 3 < P.n_val, -1002)) break;
-      const uint4 c4 = ld_stream4(P.colind + j);
-      const Vec4<T> v4 = ld_vals4<T>(P.val + j);
-      const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    // R groups of 4 nonzeros per thread per pass: their index and value loads,
+    // then all 4R x gathers in flight at once, then the products
+    constexpr int R = SPARSEP_CSR_GATHER;
+    for (uint64_t g0 = (s0 >> 2) + threadIdx.x; 4 * g0 < e0; g0 += (uint64_t)R * blockDim.x) {
+      uint32_t cc[R][4];
+      Vec4<T> v4[R];
+      bool live[R];
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (j + q >= s0 && j + q < e0) {
-          const uint64_t col = (uint64_t)it.col_off + cc[q];
-          prods[j + q - s0] = SP_BAD(P, x_ok(P, it, col), -1003) ? A(0) : mul<T>(v4.v[q], xload(xb, col, staged));
+      for (int i = 0; i < R; ++i) {
+        const uint64_t j = 4 * (g0 + (uint64_t)i * blockDim.x);
+        live[i] = j < e0 && !SP_BAD(P, j + 3 < P.n_idx && j + 3 < P.n_val, -1002);
+        if (live[i]) {
+          const uint4 c4 = ld_stream4(P.colind + j);
+          v4[i] = ld_vals4<T>(P.val + j);
+          cc[i][0] = c4.x, cc[i][1] = c4.y, cc[i][2] = c4.z, cc[i][3] = c4.w;
+        }
+      }
+      T xv[R][4];
+      uint32_t bad = 0;
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint64_t j = 4 * (g0 + (uint64_t)i * blockDim.x) + q;
+          if (live[i] && j >= s0 && j < e0) {
+            const uint64_t col = (uint64_t)it.col_off + cc[i][q];
+            if (SP_BAD(P, x_ok(P, it, col), -1003)) bad |= 1u << (4 * i + q);
+            else xv[i][q] = xload(xb, col, staged);
+          }
+        }
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint64_t j = 4 * (g0 + (uint64_t)i * blockDim.x) + q;
+          if (live[i] && j >= s0 && j < e0)
+            prods[j - s0] = (bad >> (4 * i + q)) & 1u ? A(0) : mul<T>(v4[i].v[q], xv[i][q]);
         }
     }
     __syncthreads();
