@@ -140,9 +140,15 @@ __device__ void csr_rows(const Params<T> &P, const Item &it, const T *__restrict
 #ifndef SPARSEP_CSR_GATHER
 #define SPARSEP_CSR_GATHER 1
 #endif
-constexpr int CSR_CAP = 4096;   // nonzeros per chunk
-constexpr int CSR_RCAP = 1024;  // rows per chunk
-constexpr int CSR_SHORT = 48;   // rows up to this length are summed by one thread
+#ifndef SPARSEP_CSR_CAP
+#define SPARSEP_CSR_CAP 4096
+#endif
+#ifndef SPARSEP_CSR_SHORT
+#define SPARSEP_CSR_SHORT 48
+#endif
+constexpr int CSR_CAP = SPARSEP_CSR_CAP;      // nonzeros per chunk
+constexpr int CSR_RCAP = 1024;                // rows per chunk
+constexpr int CSR_SHORT = SPARSEP_CSR_SHORT;  // rows up to this length are summed by one thread
 
 // sum of a[s, e) x over the whole CTA (thread 0 gets the total)
 template <typename T>
