@@ -453,6 +453,7 @@ def run_batch(args, dt="f32"):
         modes = [int(cands[c].mode) for c in ch if c >= 0]
         return {"matrices_rows": modes.count(0), "matrices_merge": modes.count(1),
                 "matrices_window_rows": modes.count(2), "matrices_window_merge": modes.count(3),
+                "matrices_blocks": modes.count(4),
                 "window_items": int(items[0]), "long_row_chunk_items": int(items[1])}
 
     out = {"workload": f"{len(w)} CSR matrices, rows log-uniform 1k-256k, uniform / Zipf / banded, 1-32 "
@@ -466,8 +467,9 @@ def run_batch(args, dt="f32"):
            "select_s": round(select_s, 3), "autotune_s": round(tune_s, 2), "setup_s": round(setup_s, 1),
            "chosen": {"learned": kinds(ch_learned, kinds_learned), "autotuned": kinds(ch_tuned, kinds_tuned),
                       "note": "modes 2/3 are window items: a row range whose x tile is staged in shared "
-                              "memory beside its nonzeros (a 2D tile); rows over 4096 nonzeros run as "
-                              "chunk items on many CTAs"},
+                              "memory beside its nonzeros (a 2D tile); mode 4 block items on a 4x4 BCSR "
+                              "copy (built for matrices with 4x4 block fill >= 0.25); rows "
+                              "over 4096 nonzeros run as chunk items on many CTAs"},
            "check": check,
            "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
     if cpu_s > 0:

@@ -518,6 +518,11 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
  *   mode 2, 3: as 0, 1, with window items (2D tiles): a work item whose
  *           columns span few enough rows of x has that x tile staged in
  *           shared memory with its nonzeros, and gathers from there (vec 4);
+ *   mode 4: block items on a 4 x 4 BCSR copy of the matrix (built at create
+ *           for matrices whose 4 x 4 blocks are at least a quarter full and
+ *           no block row holds more than 512 blocks): block rows dealt to the
+ *           groups, a block's 4 x rows loaded once for its 4 rows (vec 4,
+ *           pitch <= 4 * lanes); sparsep_batch_variant_applies says where;
  *   item_work: nonzero x right-hand-side products per item (0 = 65536).
  * A row longer than 4096 nonzeros runs as one work item per 4096-nonzero
  * chunk; the last chunk to finish sums the chunks' partial rows in order.
@@ -542,6 +547,8 @@ int sparsep_batch_set_x(sparsep_batch *b, uint32_t m, const void *h_x);
 int sparsep_batch_get_y(sparsep_batch *b, uint32_t m, void *h_y);
 /* change a matrix's variant; sparsep_batch_commit rebuilds the work queue */
 int sparsep_batch_set_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v);
+/* OK if variant v can run matrix m (its k; for mode 4 a BCSR copy), else ENOSYS */
+int sparsep_batch_variant_applies(const sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v);
 int sparsep_batch_get_variant(const sparsep_batch *b, uint32_t m, sparsep_batch_variant *v);
 int sparsep_batch_commit(sparsep_batch *b);
 /* the whole batch as one graph launch (NULL stream: synchronous, and the

@@ -505,6 +505,8 @@ class BatchVariant(C.Structure):
         k = row_pitch(k)
         if k % v or (int(self.mode) & 2 and v != 4):  # window modes: 4-wide variants
             return False
+        if int(self.mode) == 4:  # block items: 4-wide, one pass over the pitch (and a BCSR copy:
+            return v == 4 and self.lanes * 4 >= k  # Batch.applies checks that per matrix)
         per = -(-k // (self.lanes * v))
         acc = 1
         while acc < per:
@@ -524,6 +526,7 @@ def _batch_sigs(L):
     L.sparsep_batch_x.argtypes = [PB, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.sparsep_batch_pitch.argtypes = [PB, C.c_uint32, C.POINTER(C.c_uint32)]
     L.sparsep_batch_item_kinds.argtypes = [PB, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.sparsep_batch_variant_applies.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant)]
     L.sparsep_batch_set_x.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_get_y.argtypes = [PB, C.c_uint32, C.c_void_p]
     L.sparsep_batch_set_variant.argtypes = [PB, C.c_uint32, C.POINTER(BatchVariant)]
@@ -596,6 +599,11 @@ class Batch:
         y = np.empty((self.mats[m].s.nrows, self.nrhs[m]), dtype=self.np)
         check(lib().sparsep_batch_get_y(self.h, m, y.ctypes.data), "batch_get_y")
         return y
+
+    def applies(self, m: int, v: BatchVariant) -> bool:
+        """Whether variant v can run matrix m of this batch (block variants
+        need the matrix's BCSR copy)."""
+        return lib().sparsep_batch_variant_applies(self.h, m, C.byref(v)) == OK
 
     def item_kinds(self) -> tuple[int, int]:
         """Committed (window items, long-row chunk items)."""

@@ -29,6 +29,7 @@ struct sparsep_batch {
   std::vector<uint64_t> nnz;
   std::vector<std::vector<uint32_t>> rowptr;  // host copies: items are rebuilt without a read-back
   std::vector<std::vector<uint32_t>> clo, chi;  // per row: lowest and highest column (window items)
+  std::vector<std::vector<uint32_t>> bbrp;      // host copies of the 4 x 4 BCSR block-row pointers (if any)
   std::vector<float> feat;                    // nmats x SPARSEP_NFEATURES selector features
   std::vector<sparsep_batch_variant> var;
   std::vector<BItem> items_h;          // committed items, matrix after matrix
@@ -102,8 +103,13 @@ static uint32_t item_cap(const sparsep_batch_variant &v, uint32_t k) {
 // columns span would no longer fit the staging arena beside its nonzeros, and
 // it stages them (c0, cw) when they pay: at least two nonzeros per staged x
 // row.  Rows whose own span does not fit start ordinary items.
+static void make_block_items(const Mat<float> &M, const uint32_t *bbrp, const sparsep_batch_variant &v,
+                             uint32_t cap, std::vector<BItem> &out);
+
 static void make_items(const Mat<float> &M, const uint32_t *rowptr, const uint32_t *clo, const uint32_t *chi,
-                       uint32_t es, const sparsep_batch_variant &v, uint32_t cap, std::vector<BItem> &out) {
+                       const uint32_t *bbrp, uint32_t es, const sparsep_batch_variant &v, uint32_t cap,
+                       std::vector<BItem> &out) {
+  if (v.mode == 4) return make_block_items(M, bbrp, v, cap, out);
   const uint32_t k = M.pitch;  // every routine computes the whole padded row
   const uint32_t V = (uint32_t)std::max(1, v.vec);
   const uint32_t acc = pow2ceil((k + v.lanes * V - 1) / (v.lanes * V));
@@ -123,6 +129,7 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const uint32
   base.y = M.y;
   base.k = (uint16_t)k;
   base.ncols = M.ncols;
+  base.nrows = M.nrows;
   BItem cur{};
   bool open = false, win = false;
   uint32_t lo = 0, hi = 0;  // columns spanned by the open window item (hi exclusive; lo == hi: none yet)
@@ -190,15 +197,64 @@ static void make_items(const Mat<float> &M, const uint32_t *rowptr, const uint32
   flush();
 }
 
+// Block items of one matrix (mode 4, its 4 x 4 BCSR copy): consecutive block
+// rows up to `cap` nonzero slots (16 per block, at most BBCAP blocks) and
+// BRCAP / 4 block rows.
+static void make_block_items(const Mat<float> &M, const uint32_t *bbrp, const sparsep_batch_variant &v,
+                             uint32_t cap, std::vector<BItem> &out) {
+  const uint32_t nbr = (M.nrows + 3) / 4;
+  const uint32_t bcap = std::max<uint32_t>(1, std::min<uint32_t>(BBCAP, cap / 16));
+  BItem base{};
+  base.rowptr = M.browptr;
+  base.colind = M.bcol;
+  base.val = M.bval;
+  base.x = M.x;
+  base.y = M.y;
+  base.k = (uint16_t)M.pitch;
+  base.ncols = M.ncols;
+  base.nrows = M.nrows;
+  base.mode = MODE_BCSR;
+  base.lanes = (uint8_t)v.lanes;
+  base.vec = 4;
+  base.acc = 1;
+  BItem cur{};
+  bool open = false;
+  for (uint32_t br = 0; br < nbr; ++br) {
+    const uint32_t len = bbrp[br + 1] - bbrp[br];  // <= BBCAP (checked when the copy was built)
+    if (open && (cur.p1 - cur.p0 + len > bcap || cur.nr == BRCAP / 4)) out.push_back(cur), open = false;
+    if (!open) {
+      cur = base;
+      cur.r0 = br;
+      cur.nr = 0;
+      cur.p0 = cur.p1 = bbrp[br];
+      open = true;
+    }
+    cur.nr = (uint16_t)(br + 1 - cur.r0);
+    cur.p1 = bbrp[br + 1];
+  }
+  if (open) out.push_back(cur);
+}
+
 static int check_variant(const sparsep_batch_variant &v, uint32_t nrhs) {
-  if (v.item_work < 0 || v.mode < 0 || v.mode > 3) return SPARSEP_EINVAL;
+  if (v.item_work < 0 || v.mode < 0 || v.mode > 4) return SPARSEP_EINVAL;
   const uint32_t k = row_pitch(nrhs);
   const int V = v.vec ? v.vec : 1;
   if (v.lanes < 1 || v.lanes > 32 || (v.lanes & (v.lanes - 1))) return SPARSEP_EINVAL;
   if (V != 1 && V != 2 && V != 4) return SPARSEP_EINVAL;
   if (k % V || ((v.mode & 2) && V != 4)) return SPARSEP_ENOSYS;  // windows: 4-wide variants
+  if (v.mode == 4 && (V != 4 || (uint32_t)v.lanes * 4 < k)) return SPARSEP_ENOSYS;  // blocks: one pass of 4-wide
   if (pow2ceil((k + v.lanes * V - 1) / (v.lanes * V)) * V > (uint32_t)ACC_REGS) return SPARSEP_ENOSYS;
   return SPARSEP_OK;
+}
+
+static const uint32_t *bbrp_of(const sparsep_batch *b, uint32_t m) {
+  return b->bbrp[m].empty() ? nullptr : b->bbrp[m].data();
+}
+
+// check_variant, and block variants only where the matrix has a BCSR copy.
+static int variant_ok(const sparsep_batch *b, uint32_t m, const sparsep_batch_variant &v) {
+  if (int st = check_variant(v, b->mats_h[m].k)) return st;
+  return v.mode == 4 && !b->mats_h[m].browptr ? SPARSEP_ENOSYS : SPARSEP_OK;
 }
 
 // Merge mode, the widest vector load that divides the row pitch, and enough
@@ -238,7 +294,7 @@ static int rebuild(sparsep_batch *b) {
   b->items_h.clear();
   for (uint32_t m = 0; m < b->nmats; ++m) {
     b->item0[m] = (uint32_t)b->items_h.size();
-    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), (uint32_t)b->esize, b->var[m],
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), bbrp_of(b, m), (uint32_t)b->esize, b->var[m],
                item_cap(b->var[m], b->mats_h[m].pitch), b->items_h);
     b->nitem[m] = (uint32_t)b->items_h.size() - b->item0[m];
   }
@@ -268,6 +324,55 @@ static uint32_t grid_filling_cap(const sparsep_batch *b, uint32_t m, uint32_t ca
   return (uint32_t)std::min<uint64_t>(cap, std::max<uint64_t>(64, want));
 }
 
+// The 4 x 4 BCSR copy of matrix m for the block variants (mode 4), built on
+// the device from its uploaded CSR, for matrices whose 4 x 4 blocks are at
+// least a quarter full (selector feature 12) and whose pitch is a multiple of
+// 4; dropped again when a block row holds more than BBCAP blocks.
+template <typename T>
+static int build_blocks(sparsep_batch *b, uint32_t m) {
+  auto &h = b->mats_h[m];
+  if (!b->nnz[m] || h.pitch % 4 || b->feat[(size_t)m * SPARSEP_NFEATURES + 12] < 0.25f) return SPARSEP_OK;
+  sparsep_bcsr_layout *L = nullptr;
+  uint64_t nb = 0;
+  if (int st = sparsep_bcsr_layout_device(h.rowptr, h.colind, h.nrows, h.ncols, (uint32_t)b->nnz[m], 4, 4, &L, &nb,
+                                          b->stream))
+    return st;
+  const uint32_t nbr = (h.nrows + 3) / 4;
+  void *brp = nullptr, *bcol = nullptr, *bval = nullptr, *npb = nullptr;
+  int st = balloc(b, ((size_t)nbr + 1 + 16) * 4, &brp);
+  if (!st) st = balloc(b, (nb + 16) * 4, &bcol);
+  if (!st) st = balloc(b, (nb * 16 + 16) * sizeof(T), &bval);
+  if (!st) st = balloc(b, (nb + 16) * 4, &npb);
+  if (!st) {
+    if constexpr (std::is_same<T, float>::value)
+      st = sparsep_csr2bcsr_device_f32(L, reinterpret_cast<const float *>(h.val), (uint32_t *)brp, (uint32_t *)bcol,
+                                       (float *)bval, (uint32_t *)npb, b->stream);
+    else
+      st = sparsep_csr2bcsr_device_i32(L, reinterpret_cast<const int32_t *>(h.val), (uint32_t *)brp,
+                                       (uint32_t *)bcol, (int32_t *)bval, (uint32_t *)npb, b->stream);
+  }
+  sparsep_bcsr_layout_free(L);
+  bfree(b, npb);
+  std::vector<uint32_t> hb;
+  if (!st) {
+    hb.resize((size_t)nbr + 1);
+    st = bmap(cudaMemcpy(hb.data(), brp, hb.size() * 4, cudaMemcpyDeviceToHost));
+  }
+  uint32_t most = 0;
+  for (uint32_t i = 0; !st && i < nbr; ++i) most = std::max(most, hb[i + 1] - hb[i]);
+  if (st || most > BBCAP) {
+    bfree(b, brp);
+    bfree(b, bcol);
+    bfree(b, bval);
+    return st;
+  }
+  h.browptr = static_cast<const uint32_t *>(brp);
+  h.bcol = static_cast<const uint32_t *>(bcol);
+  h.bval = static_cast<const float *>(bval);
+  b->bbrp[m] = std::move(hb);
+  return SPARSEP_OK;
+}
+
 template <typename T>
 static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, const uint32_t *nrhs,
                         const sparsep_batch_variant *var, sparsep_batch **out) {
@@ -295,6 +400,7 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
   b->rowptr.resize(nmats);
   b->clo.resize(nmats);
   b->chi.resize(nmats);
+  b->bbrp.resize(nmats);
   for (uint32_t m = 0; m < nmats; ++m) {
     const auto *M = A[m];
     if (!M || !M->rowptr || (M->nnz && (!M->colind || !M->values))) return SPARSEP_EINVAL;
@@ -313,7 +419,8 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
     int st = balloc(b, ((size_t)M->nrows + 1 + 16) * 4, &d[0]);
     if (!st) st = balloc(b, ((size_t)M->nnz + 16) * 4, &d[1]);
     if (!st) st = balloc(b, ((size_t)M->nnz + 16) * sizeof(T), &d[2]);
-    if (!st) st = balloc(b, ((size_t)M->ncols * kp + 16) * sizeof(T), &d[3]);
+    const size_t xrows = ((size_t)M->ncols + 3) / 4 * 4;  // whole 4-column blocks (block items read them)
+    if (!st) st = balloc(b, (xrows * kp + 16) * sizeof(T), &d[3]);
     if (!st) st = balloc(b, ((size_t)M->nrows * kp + 16) * sizeof(T), &d[4]);
     if (st) return st;
     // rows longer than BCAP: a partial row per chunk and an arrival counter
@@ -333,7 +440,7 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
       BCK(cudaMemcpyAsync(d[1], M->colind, (size_t)M->nnz * 4, cudaMemcpyHostToDevice, b->stream));
       BCK(cudaMemcpyAsync(d[2], M->values, (size_t)M->nnz * sizeof(T), cudaMemcpyHostToDevice, b->stream));
     }
-    BCK(cudaMemsetAsync(d[3], 0, ((size_t)M->ncols * kp + 16) * sizeof(T), b->stream));
+    BCK(cudaMemsetAsync(d[3], 0, (xrows * kp + 16) * sizeof(T), b->stream));
     auto &h = b->mats_h[m];
     h.rowptr = (const uint32_t *)d[0];
     h.colind = (const uint32_t *)d[1];
@@ -372,11 +479,15 @@ static int batch_create(uint32_t nmats, const typename Types<T>::csr *const *A, 
       });
     for (auto &th : pool) th.join();
   }
+  for (uint32_t m = 0; m < nmats; ++m)
+    if (int st = build_blocks<T>(b, m)) return st;
+  for (uint32_t m = 0; m < nmats; ++m)
+    if (int st = variant_ok(b, m, b->var[m])) return st;
   for (uint32_t m = 0; m < nmats; ++m) {
     sparsep_batch_variant dv;
     sparsep_batch_variant_default(b->mats_h[m].k, &dv);
     b->base0[m] = (uint32_t)b->base_h.size();
-    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), (uint32_t)b->esize, dv,
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), bbrp_of(b, m), (uint32_t)b->esize, dv,
                grid_filling_cap(b, m, item_cap(dv, b->mats_h[m].pitch)), b->base_h);
     b->nbase[m] = (uint32_t)b->base_h.size() - b->base0[m];
   }
@@ -450,7 +561,7 @@ void sparsep_batch_free(sparsep_batch *b) {
 
 int sparsep_batch_set_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v) {
   if (!b || !v || m >= b->nmats) return SPARSEP_EINVAL;
-  if (int st = check_variant(*v, b->mats_h[m].k)) return st;
+  if (int st = variant_ok(b, m, *v)) return st;
   b->var[m] = *v;
   return SPARSEP_OK;
 }
@@ -557,13 +668,20 @@ int sparsep_batch_execute_one(sparsep_batch *b, uint32_t m, void *stream) {
 // the medians, 0 where a candidate does not apply; chosen (nmats) the index.
 static const sparsep_batch_variant kCand[] = {
     {0, 1, 0, 1},  {0, 1, 0, 4},  {0, 2, 0, 1},  {0, 2, 0, 4},  {0, 4, 0, 1},  {0, 4, 0, 4},
-    {0, 8, 0, 1},  {0, 8, 0, 4},  {0, 16, 0, 1}, {0, 16, 0, 4}, {0, 32, 0, 1}, {0, 32, 0, 4},
-    {1, 1, 0, 1},  {1, 1, 0, 4},  {1, 2, 0, 1},  {1, 2, 0, 4},  {1, 4, 0, 1},  {1, 4, 0, 4},
-    {1, 8, 0, 1},  {1, 8, 0, 4},  {1, 16, 0, 1}, {1, 16, 0, 4}, {1, 32, 0, 1}, {1, 32, 0, 4},
-    {2, 1, 0, 4},  {2, 2, 0, 4},  {2, 4, 0, 4},  {2, 8, 0, 4},  {2, 16, 0, 4}, {2, 32, 0, 4},
-    {3, 1, 0, 4},  {3, 2, 0, 4},  {3, 4, 0, 4},  {3, 8, 0, 4},  {3, 16, 0, 4}, {3, 32, 0, 4}};
+    {0, 8, 0, 1},  {0, 8, 0, 4},  {0, 16, 0, 1}, {0, 16, 0, 4}, {1, 1, 0, 1},  {1, 1, 0, 4},
+    {1, 2, 0, 1},  {1, 2, 0, 4},  {1, 4, 0, 1},  {1, 4, 0, 4},  {1, 8, 0, 1},  {1, 8, 0, 4},
+    {1, 16, 0, 1}, {1, 16, 0, 4}, {1, 32, 0, 4}, {2, 1, 0, 4},  {2, 2, 0, 4},  {2, 4, 0, 4},
+    {2, 8, 0, 4},  {2, 16, 0, 4}, {3, 2, 0, 4},  {3, 4, 0, 4},  {3, 8, 0, 4},  {3, 16, 0, 4},
+    {4, 1, 0, 4},  {4, 2, 0, 4},  {4, 4, 0, 4},  {4, 8, 0, 4},  {4, 16, 0, 4}, {4, 32, 0, 4}};
 constexpr int kNCand = sizeof(kCand) / sizeof(kCand[0]);
 static_assert(kNCand == SPARSEP_NVARIANTS, "the selector scores every candidate");
+
+// SPARSEP_OK if variant v can run matrix m (its k, and for block variants a
+// BCSR copy), else ENOSYS / EINVAL.
+int sparsep_batch_variant_applies(const sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v) {
+  if (!b || !v || m >= b->nmats) return SPARSEP_EINVAL;
+  return variant_ok(b, m, *v);
+}
 
 int sparsep_batch_candidates(sparsep_batch_variant *out, int max) {
   for (int i = 0; i < kNCand && out && i < max; ++i) out[i] = kCand[i];
@@ -600,10 +718,10 @@ int sparsep_batch_autotune(sparsep_batch *b, int reps, double *times_us, int32_t
 int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch_variant *v, int reps,
                                double *us_out) {
   if (!b || !v || !us_out || m >= b->nmats || reps < 1) return SPARSEP_EINVAL;
-  if (int st = check_variant(*v, b->mats_h[m].k)) return st;
+  if (int st = variant_ok(b, m, *v)) return st;
   std::vector<BItem> items;
   try {
-    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), (uint32_t)b->esize, *v,
+    make_items(b->mats_h[m], b->rowptr[m].data(), b->clo[m].data(), b->chi[m].data(), bbrp_of(b, m), (uint32_t)b->esize, *v,
                grid_filling_cap(b, m, item_cap(*v, b->mats_h[m].pitch)), items);
   } catch (const std::bad_alloc &) {
     return SPARSEP_ENOMEM;
@@ -685,14 +803,13 @@ int sparsep_batch_select(sparsep_batch *b, sparsep_selector *sel, float min_conf
   if (int st = sparsep_selector_scores(sel, b->feat.data(), b->nmats, z.data())) return st;
   for (uint32_t m = 0; m < b->nmats; ++m) {
     const float *zm = &z[(size_t)m * kNCand];
-    const uint32_t k = b->mats_h[m].k;
     int best = -1;
     float zmax = -3.0e38f;
     for (int c = 0; c < kNCand; ++c)
-      if (!check_variant(kCand[c], k) && zm[c] > zmax) zmax = zm[c], best = c;
+      if (!variant_ok(b, m, kCand[c]) && zm[c] > zmax) zmax = zm[c], best = c;
     double sum = 0.0;
     for (int c = 0; c < kNCand; ++c)
-      if (!check_variant(kCand[c], k)) sum += std::exp((double)zm[c] - zmax);
+      if (!variant_ok(b, m, kCand[c])) sum += std::exp((double)zm[c] - zmax);
     const double conf = best >= 0 ? 1.0 / sum : 0.0;
     int fb = 0;
     if (best < 0 || conf < min_confidence) {

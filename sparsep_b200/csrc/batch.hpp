@@ -17,6 +17,9 @@ template <typename T> struct Mat {
   T *y;
   T *part;         // rows longer than BCAP: their chunks' partial rows (chunks x pitch each)
   unsigned *cnt;   // and one arrival counter per such row (zero between launches)
+  const uint32_t *browptr;  // 4 x 4 BCSR copy (block variants), or null: block-row pointers,
+  const uint32_t *bcol;     // block columns,
+  const T *bval;            // 16 values per block, row-major
   uint32_t nrows, ncols, k;
   uint32_t pitch;  // x / y row pitch in elements: k rounded up to a multiple of 4 (k >= 3)
 };
@@ -42,7 +45,8 @@ constexpr uint32_t BCAP = SPARSEP_BATCH_BCAP;  // nonzeros staged per item (and 
 constexpr uint32_t BRCAP = 1024;   // rows per item
 constexpr int ACC_REGS = 8;        // V * ACC accumulators per lane
 
-enum : uint8_t { MODE_ROWS = 0, MODE_MERGE = 1, MODE_LONG = 2 };
+enum : uint8_t { MODE_ROWS = 0, MODE_MERGE = 1, MODE_LONG = 2, MODE_BCSR = 3 };
+constexpr uint32_t BBCAP = 512;   // 4 x 4 blocks staged per block item
 
 // Per-CTA staging arena (static shared memory, under the 48 KB static limit
 // with the carry rows and the barrier).  A work item's staged arrays are
@@ -82,8 +86,13 @@ struct BItem {
                     // MODE_LONG (one chunk of a row longer than BCAP): chunk c0 of cw
   void *part;       // MODE_LONG: the row's chunk partials (cw x k elements)
   unsigned *cnt;    // MODE_LONG: the row's arrival counter (the last chunk sums, resets)
+  uint32_t nrows;   // rows of the matrix (MODE_BCSR: the last block row's rows past it are not stored)
+  uint32_t pad;
 };
-static_assert(sizeof(BItem) == 88, "item layout");
+// MODE_BCSR items: rowptr / colind / val are the 4 x 4 BCSR copy's block-row
+// pointers, block columns and values; r0, nr count block rows and p0, p1 blocks.
+static_assert(sizeof(BItem) == 96, "item layout");
+static_assert(carve(BRCAP / 4, BBCAP, 64, 0).end <= ARENA, "a full block item fits the arena");
 
 // One kernel launch over items: with `head`, n CTAs claim items
 // items[0 .. n) in queue order by atomic ticket (head must be 0 at launch);

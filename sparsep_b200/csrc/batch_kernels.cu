@@ -30,6 +30,7 @@
 //   A merge-mode group streams its nonzeros in steps of U across row ends,
 //   so its loads stay U deep in flight rather than draining at every row;
 //   a rows-mode row ends with one masked step.
+//   Block items: a 4 x 4 BCSR copy of the matrix, block rows dealt to groups.
 //   Long rows (> BCAP nonzeros): one item per BCAP-nonzero chunk, the CTA's
 //     groups on contiguous parts of it; partial rows summed in chunk order
 //     by the row's last chunk to arrive.
@@ -446,6 +447,60 @@ __device__ __forceinline__ void item_merge(const View<T> &m, const Staged<T> &s,
   }
 }
 
+// Block items (4 x 4 BCSR copy): block rows dealt round-robin to groups of G
+// lanes, each lane 4 consecutive right-hand sides (pitch <= 4 G).  A block's
+// 4 x rows are loaded once for its 4 rows -- a quarter of the x gathers of the
+// same nonzeros in CSR -- two blocks per step; the block's values come from
+// shared memory 4 per load.  Each row's sum runs over its block row's blocks
+// in block-column order and within a block in column order.
+template <typename T, int G>
+__device__ __forceinline__ void item_bcsr(const BItem &it, const Staged<T> &s, int tid) {
+  using A = Acc<T>;
+  constexpr int NG = BT / G, V = 4;
+  const int gi = tid / G, gl = tid % G;
+  const uint32_t k = it.k;
+  if ((uint32_t)gl * V >= k) return;  // no barrier follows: idle lanes may leave
+  const T *xl = static_cast<const T *>(it.x) + gl * V;
+  T *yl = static_cast<T *>(it.y) + gl * V;
+  for (uint32_t lb = gi; lb < it.nr; lb += NG) {
+    A acc[4][V];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int w = 0; w < V; ++w) acc[r][w] = A(0);
+    const uint32_t q0 = s.rp[lb] - it.p0, q1 = s.rp[lb + 1] - it.p0;
+    for (uint32_t q = q0; q < q1; q += 2) {
+      const bool two = q + 1 < q1;
+      VecT<T, V> xv[2][4];
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        if (b == 0 || two) {
+          const T *xb = xl + (size_t)s.col[q + b] * 4 * k;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) xv[b][c] = ldx<T, V, false>(xb + c * k);
+        }
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        if (b == 0 || two) {
+          const T *bv = s.val + (size_t)(q + b) * 16;
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const VecT<T, 4> a4 = ldx<T, 4, true>(bv + r * 4);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+              for (int w = 0; w < V; ++w) acc[r][w] += mul<T>(a4.v[c], xv[b][c].v[w]);
+          }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t row = 4 * (it.r0 + lb) + r;
+      if (row < it.nrows) store_vec<T, V>(yl + (size_t)row * k, acc[r]);
+    }
+  }
+}
+
 // One chunk (<= BCAP nonzeros) of a row longer than BCAP; the row's chunks
 // are separate items, so a long row spreads over many SMs.  The CTA's groups
 // split the chunk's nonzeros into contiguous ranges (the row routines' vector
@@ -604,13 +659,16 @@ __global__ void __launch_bounds__(BT, MINB)
     return;
   }
   const uint32_t n = it.p1 - it.p0;
-  const bool win = it.cw != 0;
-  const Carve cv = carve(it.nr, n, sizeof(T), win ? it.cw * it.k * (uint32_t)sizeof(T) : 0);
+  const bool blocks = it.mode == MODE_BCSR;
+  const uint32_t vpe = blocks ? 16 : 1;  // values per staged entry
+  const bool win = !blocks && it.cw != 0;
+  const Carve cv = carve(it.nr, n, vpe * (uint32_t)sizeof(T), win ? it.cw * it.k * (uint32_t)sizeof(T) : 0);
   const Window w[4] = {window(it.rowptr, it.r0, it.r0 + it.nr + 1, 4), window(it.colind, it.p0, it.p1, 4),
-                       window(it.val, it.p0, it.p1, sizeof(T)),
+                       window(it.val, (uint64_t)it.p0 * vpe, (uint64_t)it.p1 * vpe, sizeof(T)),
                        win ? window(it.x, (uint64_t)it.c0 * it.k, (uint64_t)(it.c0 + it.cw) * it.k, sizeof(T))
                            : Window{0, 0, 0}};
-  if (!bchk(it.nr <= BRCAP && n <= BCAP && cv.end <= ARENA && w[0].bytes <= cv.col &&
+  if (!bchk(it.nr <= BRCAP && n <= (blocks ? BBCAP : BCAP) && cv.end <= ARENA && w[0].bytes <= cv.col &&
+                (!blocks || (w[2].lead == 0 && it.vec == 4 && (uint32_t)it.lanes * 4 >= it.k)) &&
                 w[1].bytes <= cv.val - cv.col && w[2].bytes <= cv.xw - cv.val &&
                 (!win || (w[3].bytes <= cv.end - cv.xw && w[3].lead == 0 && it.vec == 4 &&
                           (uint64_t)it.c0 + it.cw <= it.ncols)),
@@ -630,7 +688,19 @@ __global__ void __launch_bounds__(BT, MINB)
 #ifdef SPARSEP_CHECK
     for (uint32_t i = tid; i < it.nr; i += BT) rp_ok = rp_ok && s.rp[i] <= s.rp[i + 1];
 #endif
-    if (!staged_ok(col, n, it.c0, win ? it.cw : it.ncols, win, bchk(rp_ok, err, -2105), err, -2106)) return;
+    const uint32_t bound = blocks ? (it.ncols + 3) / 4 : win ? it.cw : it.ncols;  // block columns, or columns
+    if (!staged_ok(col, n, it.c0, bound, win, bchk(rp_ok, err, -2105), err, -2106)) return;
+  }
+  if (blocks) {
+    switch (it.lanes) {
+      case 1: item_bcsr<T, 1>(it, s, tid); break;
+      case 2: item_bcsr<T, 2>(it, s, tid); break;
+      case 4: item_bcsr<T, 4>(it, s, tid); break;
+      case 8: item_bcsr<T, 8>(it, s, tid); break;
+      case 16: item_bcsr<T, 16>(it, s, tid); break;
+      default: item_bcsr<T, 32>(it, s, tid); break;
+    }
+    return;
   }
   if (win) {
     const View<T> m{reinterpret_cast<const T *>(sh.arena + cv.xw), static_cast<T *>(it.y), it.k, it.cw};

@@ -69,8 +69,7 @@ def test_batch_every_candidate(dtype):
     for v in sp.capi.batch_candidates():
         applied = False
         for m, d in enumerate(data):
-            k = d[4]
-            if v.applies(k):
+            if b.applies(m, v):
                 b.set_variant(m, v)
                 applied = True
         if not applied:
@@ -108,7 +107,7 @@ def test_batch_wide_rhs(dtype):
     b.execute()
     check_batch(b, mats, data, dtype)
     for v in sp.capi.batch_candidates():
-        if not all(v.applies(d[4]) for d in data):
+        if not all(b.applies(m, v) for m in range(len(data))):
             continue
         for m in range(len(data)):
             b.set_variant(m, v)
@@ -159,7 +158,7 @@ def test_batch_long_rows(dtype):
     check_batch(b, mats, data, dtype)
     for v in sp.capi.batch_candidates()[::5]:
         for m, d in enumerate(data):
-            if v.applies(d[4]):
+            if b.applies(m, v):
                 b.set_variant(m, v)
         b.commit()
         b.execute()
@@ -194,12 +193,82 @@ def test_batch_window_items(dtype):
     for m, d in enumerate(data):
         b.set_x(m, d[5])
     for v in sp.capi.batch_candidates():
-        if not v.mode & 2 or not any(v.applies(d[4]) for d in data):
+        if not v.mode & 2 or not any(b.applies(m, v) for m in range(len(data))):
             continue
         for m, d in enumerate(data):
-            b.set_variant(m, v if v.applies(d[4]) else sp.capi.BatchVariant(1, 8, 0, 4))
+            b.set_variant(m, v if b.applies(m, v) else sp.capi.BatchVariant(1, 8, 0, 4))
         b.commit()
         nwin, _ = b.item_kinds()
         assert nwin > 0
         b.execute()
         check_batch(b, mats, data, dtype)
+
+
+def block_matrix(rng, n, dtype, fill=0.8, half_bw=6):
+    """Square matrix of 4 x 4 blocks around the diagonal (block columns within
+    half_bw of the block row, each block's entries present with probability
+    fill), n not a multiple of 4: the last block row and column are partial."""
+    nb = (n + 3) // 4
+    rows, cols = [], []
+    for br in range(nb):
+        for bc in range(max(0, br - half_bw), min(nb, br + half_bw + 1)):
+            if rng.random() < 0.5:
+                continue
+            mask = rng.random((4, 4)) < fill
+            rr, cc = np.nonzero(mask)
+            rr, cc = rr + 4 * br, cc + 4 * bc
+            ok = (rr < n) & (cc < n)
+            rows.append(rr[ok])
+            cols.append(cc[ok])
+    r = np.concatenate(rows).astype(np.int64)
+    c = np.concatenate(cols).astype(np.int64)
+    key = np.unique(r * n + c)
+    r, c = key // n, key % n
+    rp = np.zeros(n + 1, dtype=np.uint32)
+    np.cumsum(np.bincount(r, minlength=n), out=rp[1:])
+    np_t = capi.DTYPES[dtype].np
+    vv = (rng.uniform(-1, 1, c.size) if dtype == "f32" else rng.integers(-8, 9, c.size)).astype(np_t)
+    return rp, c.astype(np.uint32), vv
+
+
+@pytest.mark.parametrize("dtype", ["f32", "i32"])
+def test_batch_block_items(dtype):
+    """Block-structured matrices get a 4 x 4 BCSR copy and run under every
+    block variant (mode 4) that fits their k, partial last blocks included;
+    a scattered matrix gets none.  Every column against the oracle, then the
+    autotuner over all candidates."""
+    rng = np.random.default_rng(13)
+    data = []
+    for n, k in ((4001, 4), (2002, 16), (3003, 7), (1501, 32), (999, 12)):
+        rp, ci, vv = block_matrix(rng, n, dtype)
+        x = (rng.uniform(-1, 1, (n, k)) if dtype == "f32" else rng.integers(-8, 9, (n, k))).astype(
+            capi.DTYPES[dtype].np)
+        data.append((n, rp, ci, vv, k, x))
+    n = 3000
+    rp, ci, vv = sp.synth.batch_matrix(rng, n, "uniform", capi.DTYPES[dtype].np)
+    data.append((n, rp, ci, vv, 8, rng.integers(-8, 9, (n, 8)).astype(capi.DTYPES[dtype].np)))
+    mats = [sp.csr(dtype, n, n, rp, ci, vv) for (n, rp, ci, vv, k, x) in data]
+    b = sp.capi.Batch(dtype, mats, [d[4] for d in data])
+    for m, d in enumerate(data):
+        b.set_x(m, d[5])
+    blocks = [v for v in sp.capi.batch_candidates() if v.mode == 4]
+    assert len(blocks) == 6
+    assert not any(b.applies(len(data) - 1, v) for v in blocks)  # no copy for the scattered matrix
+    for m in range(len(data) - 1):
+        assert any(b.applies(m, v) for v in blocks), m
+    ran = 0
+    for v in blocks:
+        use = [m for m in range(len(data)) if b.applies(m, v)]
+        if not use:
+            continue
+        for m in range(len(data)):
+            b.set_variant(m, v if m in use else sp.capi.BatchVariant(1, 8, 0, 4 if data[m][4] % 4 == 0 else 1))
+        b.commit()
+        b.execute()
+        check_batch(b, mats, data, dtype)
+        ran += len(use)
+    assert ran >= 10
+    b.autotune(reps=1)
+    b.execute()
+    check_batch(b, mats, data, dtype)
+    b.status()
