@@ -88,7 +88,10 @@ static uint32_t pow2ceil(uint32_t v) {
   return p;
 }
 
-static constexpr uint32_t DEFAULT_ITEM_WORK = 65536;  // nonzero x right-hand-side products per item
+#ifndef SPARSEP_BATCH_ITEM_WORK
+#define SPARSEP_BATCH_ITEM_WORK 65536
+#endif
+static constexpr uint32_t DEFAULT_ITEM_WORK = SPARSEP_BATCH_ITEM_WORK;  // nonzero x right-hand-side products per item
 
 // Nonzeros per item for a variant: about item_work products, within [32, BCAP].
 static uint32_t item_cap(const sparsep_batch_variant &v, uint32_t k) {

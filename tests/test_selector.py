@@ -224,7 +224,7 @@ def test_batch_select_results_and_fallback(dtype):
     ch, fb = b.select(sel, min_confidence=0.0)
     assert (fb == 0).all() and (ch >= 0).all()
     cand = capi.batch_candidates()
-    assert all(cand[c].applies(d[4]) for c, d in zip(ch, data))
+    assert all(cand[c].applies(d[4]) and b.applies(m, cand[c]) for m, (c, d) in enumerate(zip(ch, data)))
     b.execute()
     check_batch(b, mats, data, dtype)
     ch2, fb2 = b.select(sel, min_confidence=1.01, reps=1)
