@@ -469,7 +469,7 @@ def run_batch(args, dt="f32"):
                       "note": "modes 2/3 are window items: a row range whose x tile is staged in shared "
                               "memory beside its nonzeros (a 2D tile); mode 4 block items on a 4x4 BCSR "
                               "copy (built for matrices with 4x4 block fill >= 0.25); rows "
-                              "over 4096 nonzeros run as chunk items on many CTAs"},
+                              "over 5120 nonzeros run as chunk items on many CTAs"},
            "check": check,
            "gpu_launches_per_step": {"plain": len(w), "queue": 1}}
     if cpu_s > 0:

@@ -506,7 +506,7 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
  * ncols x k and y nrows x k, row-major; on the device their rows are `pitch`
  * elements apart, k rounded up to a multiple of 4 for k >= 3, so that 4-wide
  * loads serve every k), multiplied by ONE kernel launch:
- * its CTAs claim work items (row ranges of any matrix, at most 4096 nonzeros,
+ * its CTAs claim work items (row ranges of any matrix, at most 5120 nonzeros,
  * or one longer row) from a device work queue by atomic ticket, replayed as a
  * CUDA graph (queue reset + kernel).  The row routine of each matrix is a
  * variant: the CTA is cut into groups of `lanes` (1..32, power of two) lanes,
@@ -523,8 +523,8 @@ int sparsep_partition_block_rows(const uint32_t *browptr, uint32_t num_block_row
  *           no block row holds more than 512 blocks): block rows dealt to the
  *           groups, a block's 4 x rows loaded once for its 4 rows (vec 4,
  *           pitch <= 4 * lanes); sparsep_batch_variant_applies says where;
- *   item_work: nonzero x right-hand-side products per item (0 = 65536).
- * A row longer than 4096 nonzeros runs as one work item per 4096-nonzero
+ *   item_work: nonzero x right-hand-side products per item (0 = 163840).
+ * A row longer than 5120 nonzeros runs as one work item per 5120-nonzero
  * chunk; the last chunk to finish sums the chunks' partial rows in order.
  * FP32 and INT32 (integers wrap exactly, as the single-vector path).  Status
  * ENOSYS: the variant does not apply to that k. */
@@ -576,8 +576,8 @@ int sparsep_batch_time_variant(sparsep_batch *b, uint32_t m, const sparsep_batch
                                double *us_out);
 int sparsep_batch_get_info(const sparsep_batch *b, uint64_t *compulsory_bytes, uint64_t *items, uint64_t *nnz);
 /* committed work items by kind: window items (a row range with its x tile
- * staged in shared memory) and chunk items (rows longer than 4096 nonzeros,
- * one item per 4096-nonzero chunk) */
+ * staged in shared memory) and chunk items (rows longer than 5120 nonzeros,
+ * one item per 5120-nonzero chunk) */
 int sparsep_batch_item_kinds(const sparsep_batch *b, uint64_t *window_items, uint64_t *chunk_items);
 
 /* ------------------------------------------------------------------------ */

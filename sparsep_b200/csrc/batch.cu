@@ -89,7 +89,7 @@ static uint32_t pow2ceil(uint32_t v) {
 }
 
 #ifndef SPARSEP_BATCH_ITEM_WORK
-#define SPARSEP_BATCH_ITEM_WORK 65536
+#define SPARSEP_BATCH_ITEM_WORK 163840
 #endif
 static constexpr uint32_t DEFAULT_ITEM_WORK = SPARSEP_BATCH_ITEM_WORK;  // nonzero x right-hand-side products per item
 

@@ -32,7 +32,7 @@ constexpr uint32_t row_pitch(uint32_t k) { return k <= 2 ? k : (k + 3) & ~3u; }
 
 constexpr int BT = 256;            // threads per CTA
 #ifndef SPARSEP_BATCH_BCAP
-#define SPARSEP_BATCH_BCAP 4096
+#define SPARSEP_BATCH_BCAP 5120
 #endif
 #ifndef SPARSEP_BATCH_ARENA
 #define SPARSEP_BATCH_ARENA 48000

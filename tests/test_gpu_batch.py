@@ -117,12 +117,12 @@ def test_batch_wide_rhs(dtype):
 
 
 def long_row_batch(dtype, seed=11):
-    """Matrices whose longest rows exceed one 4096-nonzero chunk (4097 up to
-    50,000 nonzeros, so 2..13 chunk items per row) beside ordinary rows, with
+    """Matrices whose longest rows exceed one 5120-nonzero chunk (5121 up to
+    50,000 nonzeros, so 2..10 chunk items per row) beside ordinary rows, with
     k = 1, 3, 16 and 33 right-hand sides."""
     rng = np.random.default_rng(seed)
     out = []
-    for m, (k, long_lens) in enumerate(((1, (4097, 9000)), (3, (8192, 50000)), (16, (12289,)), (33, (4097, 20000)))):
+    for m, (k, long_lens) in enumerate(((1, (5121, 9000)), (3, (10240, 50000)), (16, (15361,)), (33, (5121, 20000)))):
         n = 60_000
         lens = rng.integers(1, 40, n)
         rows = rng.choice(n, len(long_lens), replace=False)
@@ -149,8 +149,8 @@ def test_batch_long_rows(dtype):
     b = sp.capi.Batch(dtype, mats, [d[4] for d in data])
     for m, d in enumerate(data):
         b.set_x(m, d[5])
-    assert b.item_kinds()[1] == sum(-(-int(l) // 4096) for d in data for l in np.diff(d[1].astype(np.int64))
-                                    if l > 4096)
+    assert b.item_kinds()[1] == sum(-(-int(l) // 5120) for d in data for l in np.diff(d[1].astype(np.int64))
+                                    if l > 5120)
     for _ in range(3):
         b.execute()
         check_batch(b, mats, data, dtype)
